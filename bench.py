@@ -1,0 +1,328 @@
+#!/usr/bin/env python
+"""Benchmark of the coupled explicit phase-field step on B200.
+
+One bench "step" = one time step of the reference's loop (principal.f90:93-226:
+temperatura, two phase sweeps, solute, M0, swap) over the whole domain.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+ours       value = GCell-updates/s of the fused FP64 step, device-resident
+           (CUDA events, max over ranks); e2e = the same job through the C-ABI
+           with the state uploaded from / downloaded to pinned host memory and
+           a per-step probe read; roofline of the dominant kernel from CUDA
+           events around each launch; cpu_baseline = the CPU oracle on a
+           bounded sample (rank 0, N = 1).
+reference  the reference's CPU path, i.e. the CPU oracle (C restatement of
+           the Fortran OpenMP path; the Fortran cannot be compiled here) on all
+           host threads, rank 0 only.
+Multi-GPU: the path shards by domain (replicas only): every rank runs its own
+domain, no data-path collective; value = all ranks' cell updates / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "phase-field-project-3d_b200"))
+
+METRIC = "GCell-updates/s & %HBM peak, FP32 vs FP64 plain; p50/p99 batched-solve latency"
+UNIT = "GCell-updates/s"
+# algorithmic HBM bytes per cell and step of the fused step: phi, c, T, DPP
+# each read once and written once (8 B FP64 / 4 B FP32)
+STEP_BYTES_PER_CELL = {64: 64, 32: 32}
+# algorithmic bytes per cell of each fused pass:
+#   first = temperatura + sweep 1: reads phi, c, DPP; writes T, phi_mid
+#   last  = sweep 2 + solute     : reads phi_mid, c; writes phi, DPP, c
+PASS_BYTES_PER_CELL = {64: 40, 32: 20}
+CPU_SAMPLE = (512, 512, 32)   # bounded CPU sample: bottom slab of the workload
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str, precision: int):
+    """Per-cell DRAM bytes of a fused pass from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    try:
+        for line in open(path):
+            t = line.split()
+            if len(t) >= 3 and t[0] == kernel and t[1] == f"fp{precision}":
+                return float(t[2].split("=")[1])
+    except Exception:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.idx = gpu_index
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if len(r) > 8]
+        mx = max(float(r[2]) for r in rows if len(r) > 8)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) > 8:
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+        loaded = [s for s in sm if s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def cpu_oracle_rate(precision_unused: int, seconds: float, warmup: int = 1, min_steps: int = 2):
+    """GCell-updates/s of the CPU oracle on the bounded sample (all host threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from pf3d import deck, init
+    w = deck.WORKLOADS["c2_512x512x1024_fp64"]
+    nx, ny, nz = CPU_SAMPLE
+    p = w.params()
+    g = deck.grid(nx, ny, nz, w.dx)
+    st = init.initial_state(nx, ny, nz, w.n_bumps, w.seed, p)
+    o = pyoracle.Oracle(g, p)
+    o.load_state(st)
+    o.step(warmup)
+    n, t0 = 0, time.perf_counter()
+    while n < min_steps or time.perf_counter() - t0 < seconds:
+        o.step(1)
+        n += 1
+    dt = time.perf_counter() - t0
+    return (nx * ny * nz * n / dt / 1e9, n, dt, pyoracle.num_threads())
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from pf3d import deck, init
+    w = deck.WORKLOADS[args.workload]
+    nx, ny, nz = CPU_SAMPLE
+    p = w.params()
+    g = deck.grid(nx, ny, nz, w.dx)
+    st = init.initial_state(nx, ny, nz, w.n_bumps, w.seed, p)
+    o = pyoracle.Oracle(g, p)
+    o.load_state(st)
+    o.step(args.warmup)
+    t0 = time.perf_counter()
+    o.step(args.steps)
+    dt = time.perf_counter() - t0
+    v = nx * ny * nz * args.steps / dt / 1e9
+    threads = pyoracle.num_threads()
+    sample = (f"{nx}x{ny}x{nz} bottom slab of the {w.nx}x{w.ny}x{w.nz} workload (same deck and seeded "
+              f"initial state), {args.steps} steps after {args.warmup} warm-up")
+    line = {
+        "metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": w.name, "cells": w.cells, "sample_cells": nx * ny * nz},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference CPU OpenMP path as the C restatement in oracle/ (no Fortran compiler in the image)",
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="c2_512x512x1024_fp64")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import pf3d
+    from pf3d import deck, init
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    w = deck.WORKLOADS[args.workload]
+    g, p = w.grid(), w.params()
+    prec = w.precision
+    cells = w.cells
+    st = init.initial_state(w.nx, w.ny, w.nz, w.n_bumps, w.seed + rank, p)
+    stream = torch.cuda.current_stream()
+
+    dom = pf3d.Domain(g, p, prec)
+    dom.set_stream(stream.cuda_stream)
+    dom.load_state(st)
+    dom.step(args.warmup)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        dom.step(1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    clk = clocks.stop()
+    value = cells * args.steps * world / (ms / 1e3) / 1e9
+    launches_per_step = 2 if p.n_varreduras >= 2 else 1
+    launches_per_step += max(0, p.n_varreduras - 2)
+
+    # ---- per-kernel timing (CUDA events around every fused launch, same stream) ----
+    dom.set_option(pf3d.PF_OPT_KTIMING, 1)
+    dom.kernel_times(reset=True)
+    dom.step(args.steps)
+    nf, mf, nl, ml = dom.kernel_times(reset=True)
+    dom.set_option(pf3d.PF_OPT_KTIMING, 0)
+    peak, peak_kind = measured_peaks()
+    kname, n_k, ms_k = ("fused_first", nf, mf) if mf >= ml else ("fused_last", nl, ml)
+    alg_bytes = PASS_BYTES_PER_CELL[prec] * cells
+    avg_s = ms_k / max(1, n_k) / 1e3
+    achieved = alg_bytes / avg_s / 1e9
+    tr = ncu_traffic(kname, prec)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": (tr * cells if tr is not None else None), "kernel": kname,
+                "kernel_ms": avg_s * 1e3, "peak_source": f"{peak_kind} hbm_gbs",
+                "shares": {"fused_first": mf / max(1e-9, mf + ml), "fused_last": ml / max(1e-9, mf + ml)}}
+    step_hbm_frac = value / world * STEP_BYTES_PER_CELL[prec] / peak
+
+    # ---- end to end through the C-ABI with pinned host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        host = {k: torch.from_numpy(st[k]).pin_memory() for k in ("phi", "c", "T")}
+        host["dpp"] = torch.zeros(st["phi"].shape, dtype=torch.float64).pin_memory()
+        out = {k: torch.empty_like(v).pin_memory() for k, v in host.items()}
+        fields_in = [("phase_field_old", "phi"), ("conc_soluto_old", "c"), ("TOLD", "T"), ("DPP", "dpp")]
+        dom2 = pf3d.Domain(g, p, prec)
+        dom2.set_stream(stream.cuda_stream)
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        for fname, key in fields_in:
+            dom2.upload(fname, host[key].numpy())
+        probe = 0.0
+        for _ in range(args.steps):
+            dom2.step(1)
+            # the reference's per-sweep progress print reads 2 cells per sweep
+            probe += dom2.probe("phase_field_old", w.nx // 2, 10, max(w.nz // 2, 1))
+            probe += dom2.probe("phase_field_old", w.nx // 2, min(100, w.ny - 1), max(w.nz // 2, 1))
+        for fname, key in fields_in:
+            dom2.download(fname, out[key].numpy())
+        torch.cuda.synchronize()
+        t_e2e = max_over_ranks(time.perf_counter() - t0)
+        barrier()
+        dom2.close()
+        state_bytes = 4 * cells * 8
+        e2e = {"value": cells * args.steps * world / t_e2e / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": state_bytes / args.steps,
+               "d2h_bytes_per_step": state_bytes / args.steps + 2 * 8,
+               "job": "upload 4 state fields, K steps with a 2-cell probe read each, download 4 fields"}
+        del host, out
+
+    dom.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, n, dt, thr = cpu_oracle_rate(prec, args.cpu_seconds)
+        nx, ny, nz = CPU_SAMPLE
+        cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
+               "sample": f"{nx}x{ny}x{nz} bottom slab of the workload, {n} steps in {dt:.1f} s "
+                         f"(C restatement of the reference CPU OpenMP path)"}
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if prec == 64 else "f32", "data": "synthetic",
+        "config": {"workload": w.name, "grid": [w.nx, w.ny, w.nz], "cells": cells, "precision": f"fp{prec}",
+                   "sweeps_per_step": p.n_varreduras, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (resident state of 4 fields x 8 B x 268M cells)"},
+        "hbm_frac_step": step_hbm_frac,
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,200 @@
+/*
+ * pf3d.h -- C-ABI of the B200 implementation of the coupled explicit time step
+ * of the 3-D Al-Cu phase-field model (ileaof/phase-field-project-3D).
+ *
+ * The reference's hot path is a set of argument-less Fortran subroutines that
+ * act on module globals (source/variaveis.f90:3-50), called in a fixed order
+ * from the time loop in source/principal.f90:93-259.  This header exports one
+ * entry point per subroutine (same name, same meaning), plus a fused step and
+ * batched / pooled entry points.  A Fortran caller binds these through
+ * ISO_C_BINDING (bind(C), c_loc of its module arrays); a C/C++/Python caller
+ * uses them directly.  Plain pointers and sizes only: no CUDA or torch types.
+ *
+ * Conventions
+ *   - Every function returns 0 on success, a negative PF_E* code otherwise;
+ *     pf_last_error() gives the message.
+ *   - Fields are Nx*Ny*Nz arrays in Fortran order (i fastest), 1-based (i,j,k)
+ *     in every index argument, exactly like the reference arrays.
+ *   - A context owns its device buffers; the caller owns host arrays.
+ *   - Each context is driven by one host thread (the reference calls its
+ *     subroutines from serial code only) and runs on one CUDA stream.
+ *   - Work is stream-ordered; pf_download, pf_diagnosticos, pf_probe and
+ *     pf_sync block until the result is on the host.
+ */
+#ifndef PF3D_H
+#define PF3D_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PF3D_VERSION 1
+
+/* status codes */
+#define PF_OK 0
+#define PF_E_ARG (-1)      /* invalid argument / unsupported size          */
+#define PF_E_CUDA (-2)     /* CUDA runtime error (message in pf_last_error) */
+#define PF_E_NOMEM (-3)    /* device allocation refused or over budget      */
+#define PF_E_STATE (-4)    /* call not valid in the current state           */
+#define PF_E_NODEV (-5)    /* no CUDA device visible                        */
+
+/* field ids: the seven resident arrays of source/principal.f90:61-63 */
+#define PF_PHASE_OLD 0     /* phase_field_old */
+#define PF_PHASE_NEW 1     /* phase_field_new */
+#define PF_CONC_OLD 2      /* conc_soluto_old */
+#define PF_CONC_NEW 3      /* conc_soluto_new */
+#define PF_TOLD 4          /* TOLD            */
+#define PF_TNEW 5          /* TNEW            */
+#define PF_DPP 6           /* DPP             */
+
+/* storage / arithmetic precision of a context */
+#define PF_FP64 64         /* plain form: FP64 end to end, reference arithmetic  */
+#define PF_FP32 32         /* FP32 fields and stencils, FP64 scalars and sums    */
+
+/* boundary treatment */
+#define PF_BC_REFERENCE 0  /* plane-copy decoration of the reference (default)   */
+
+/* Grid: Nx, Ny, Nz (>= 5 each) and the spacings dx, dy, dz [m]. */
+typedef struct pf_grid {
+    int nx, ny, nz;
+    double dx, dy, dz;
+} pf_grid;
+
+/*
+ * Physical and numerical parameters: the entrada.dat deck, by the reference's
+ * names (source/entrada.f90:19-89).  Ke, Sigma, Beta and ajuste are REAL(4)
+ * in the reference (source/variaveis.f90:28) and stay float here, because
+ * their single-precision rounding enters W0/E0 and M0.
+ */
+typedef struct pf_params {
+    double Tm;             /* melting temperature [K]                             */
+    double T0;             /* initial temperature [K]                             */
+    double delta_H;        /* latent heat [J/m^3]                                 */
+    double M0;             /* interface mobility used by step 1 (then auxiliar)   */
+    double Cp_s;           /* heat capacity used by temperatura (cp = cp_s)       */
+    double D;              /* heat-equation diffusivity; the reference never
+                              assigns its module variable D, so the deck value 0
+                              reproduces it                                       */
+    double AAA;            /* noise amplitude as read from the deck (before the
+                              dt rescale of entrada.f90:179-185)                  */
+    double DELTA_EPSLON;   /* anisotropy strength                                 */
+    double D_sol, D_liq;   /* solute diffusivities [m^2/s]                        */
+    float  Ke;             /* partition coefficient (REAL(4))                     */
+    double Me;             /* liquidus slope [K/mol fraction]                     */
+    double Vm;             /* molar volume [m^3/mol]                              */
+    double R;              /* gas constant                                        */
+    double C0;             /* initial solute concentration                        */
+    double Thin_Interface; /* Lambda = Thin_Interface * dx                        */
+    float  Sigma;          /* surface energy (REAL(4))                            */
+    float  Beta;           /* kinetic coefficient (REAL(4))                       */
+    float  ajuste;         /* mobility adjustment (REAL(4))                       */
+    double TP;             /* isothermal TP line; replaced by T0 if taxa_resfr>0   */
+    double taxa_resfr;     /* cooling rate [K/s]; TP = T0 - taxa*dt*it            */
+    int    n_varreduras;   /* phase sweeps per step (>= 1)                        */
+    int    h_quintico;     /* 1 = quintic h(phi), 0 = cubic                       */
+    int    ruido_tipo;     /* 0 cell noise >= 0, 1 zero-mean cell, 2 smooth       */
+    int    bc;             /* PF_BC_REFERENCE                                     */
+    double stoptime;       /* [s]; 0 = no stop test (driver only)                 */
+    int    WriteFileD_timeCounter; /* output cadence (driver only)               */
+} pf_params;
+
+/* Quantities derived once at set-up (entrada.f90:159-185, W0_E0.f90). */
+typedef struct pf_derived {
+    double DELTA_T;        /* dt = dx^2 / (7.5 D_liq)                             */
+    double AAA;            /* effective noise amplitude after the dt rescale      */
+    double Lambda;         /* Thin_Interface * dx                                 */
+    double W0, E0;         /* from the W0_E0 fixed-point scan                     */
+    long   w0e0_iterations;
+} pf_derived;
+
+/* Host-side step state that the reference keeps in module scalars. */
+typedef struct pf_state {
+    int    it;             /* last completed step (0 before the first)            */
+    double TP;             /* current TP                                          */
+    double M0;             /* mobility the next phase sweep will use              */
+    double Cs_eq, Cl_eq;   /* from the last phase sweep                           */
+    float  time;           /* REAL(4) simulated time (principal.f90:96)           */
+} pf_state;
+
+typedef struct pf_ctx pf_ctx;
+
+/* ---- library / context lifecycle ------------------------------------- */
+int         pf_version(void);
+const char* pf_last_error(const pf_ctx* ctx);   /* ctx may be NULL           */
+/* Bytes of device memory a context of this grid and precision holds.       */
+long long   pf_ctx_bytes(const pf_grid* g, int precision);
+int pf_create(const pf_grid* g, const pf_params* p, int precision, pf_ctx** out);
+int pf_destroy(pf_ctx* ctx);
+int pf_get_derived(const pf_ctx* ctx, pf_derived* out);
+int pf_get_state(const pf_ctx* ctx, pf_state* out);
+int pf_set_state(pf_ctx* ctx, const pf_state* st);
+int pf_sync(pf_ctx* ctx);
+/* Run the context's work on the caller's CUDA stream (a cudaStream_t passed
+   as void*; NULL returns to the context's own stream).                     */
+int pf_set_stream(pf_ctx* ctx, void* stream);
+
+/* options (pf_set_option / pf_get_option) */
+#define PF_OPT_FUSED 1     /* 1 (default): pf_step uses the fused kernels;
+                              0: it calls the per-subroutine kernels        */
+#define PF_OPT_TILE_Y 2    /* fused tile height: 4, 8 (default) or 16       */
+#define PF_OPT_ZCHUNK 3    /* z planes per fused CTA (0 = whole column)     */
+#define PF_OPT_KTIMING 4   /* 1: time every fused launch with CUDA events   */
+int pf_set_option(pf_ctx* ctx, int opt, int value);
+int pf_get_option(const pf_ctx* ctx, int opt, int* value);
+/* With PF_OPT_KTIMING on: launches and summed device milliseconds of the
+   first (heat + sweep 1) and last (sweep 2 + solute) fused kernels since
+   the last reset.  Synchronises the context's stream.                      */
+int pf_kernel_times(pf_ctx* ctx, long* n_first, double* ms_first, long* n_last, double* ms_last, int reset);
+
+/* ---- data residency (principal.f90:60-64, :182, :248, :268-272) ---------- */
+/* host array: Nx*Ny*Nz doubles, Fortran order.  FP32 contexts convert.     */
+int pf_upload(pf_ctx* ctx, int field, const double* host);
+int pf_download(pf_ctx* ctx, int field, double* host);
+/* read one cell, 1-based (the progress print of equacao_campo_fase.f90:174) */
+int pf_probe(pf_ctx* ctx, int field, int i, int j, int k, double* value);
+
+/* ---- host scalar set-up, FP64 (no device needed) ---------------------- */
+/* W0_E0.f90:10-31: fixed-point scan for W0 and E0.                        */
+int pf_w0_e0(const pf_grid* g, const pf_params* p, double* W0, double* E0, long* iterations);
+/* auxiliar.f90:12-42: M0 from TP and the equilibrium compositions.        */
+int pf_auxiliar_scalar(const pf_params* p, double E0, double W0, double TP,
+                       double Cs_eq, double Cl_eq, double* M0);
+
+/* ---- one entry point per reference subroutine ------------------------- */
+/* temperatura.f90: TNEW = TOLD, then temp_body.inc on 2..N-1, with the
+   given TP (the reference passes the TP of the previous step).            */
+int pf_temperatura(pf_ctx* ctx, double TP);
+/* equacao_campo_fase.f90: Cs_eq/Cl_eq from TP, phase_field_new = old,
+   phase_body.inc on 3..N-2 (noise index it), boundary decoration.  Cs_eq
+   and Cl_eq may be NULL.                                                  */
+int pf_equacao_campo_fase(pf_ctx* ctx, int it, double TP, double M0,
+                          double* Cs_eq, double* Cl_eq);
+/* principal.f90:128-150: phase_field_old = phase_field_new (between sweeps) */
+int pf_copy_phase_new_to_old(pf_ctx* ctx);
+/* concentracao_soluto.f90: conc_body.inc on 2..N-1, conc_soluto_old = new,
+   boundary decoration of conc_soluto_new from conc_soluto_old.            */
+int pf_concentracao_soluto(pf_ctx* ctx);
+/* auxiliar.f90 with the context's E0/W0/parameters.                       */
+int pf_auxiliar(const pf_ctx* ctx, double TP, double Cs_eq, double Cl_eq, double* M0);
+/* diagnosticos.f90: out = {L2_phi, phi_max, phi_min, solute_total,
+   free_energy} of phase_field_new / conc_soluto_new.                      */
+int pf_diagnosticos(pf_ctx* ctx, double out[5]);
+/* principal.f90:200-226: old <- new for phi, T and c.  Done by exchanging
+   buffers: afterwards the "new" arrays hold the previous "old" data until
+   the next subroutine overwrites them (the reference's loop reads none of
+   them in between).                                                        */
+int pf_swap(pf_ctx* ctx);
+
+/* ---- fused step ------------------------------------------------------- */
+/* Runs n_steps whole iterations of principal.f90:93-226 (temperatura, TP
+   ramp, n_varreduras sweeps, solute, auxiliar, swap) with the fused
+   kernels, starting from the context's pf_state.  Results equal the
+   sequence of per-subroutine calls above.                                 */
+int pf_step(pf_ctx* ctx, int n_steps);
+/* Same, and also fills out[5] with the diagnostics of the final state.    */
+int pf_step_diag(pf_ctx* ctx, int n_steps, double out[5]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PF3D_H */

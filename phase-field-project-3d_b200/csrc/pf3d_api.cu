@@ -1,0 +1,606 @@
+// pf3d_api.cu -- C-ABI of the B200 phase-field step (include/pf3d.h).
+//
+// A pf_ctx is one domain resident in HBM: the seven fields of the
+// reference (principal.f90:61-63) in pitched FP64 or FP32 storage, one
+// stream, and the host scalars the reference keeps in module variables
+// (TP, M0, it, time).  The per-subroutine entry points launch the
+// one-thread-per-cell kernels; pf_step launches the fused z-marching passes.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+#include "../../include/pf3d.h"
+#include "pf3d_launch.h"
+#include "pf3d_scalar.h"
+
+using namespace pf3d;
+
+namespace {
+std::mutex g_err_mu;
+std::string g_err;   // last error of calls without a context
+
+int set_global_err(int code, const std::string& msg)
+{
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    g_err = msg;
+    return code;
+}
+}  // namespace
+
+struct pf_ctx {
+    pf_grid g;
+    pf_params p;
+    int prec;          // 64 or 32
+    size_t es;         // element size
+    pf_derived dv;
+    pf_state st;
+    DomainDesc dd;
+    void* fld[7];      // device pointer of each field id
+    void* base;
+    size_t field_bytes;
+    double* d_part;
+    int nblk;
+    double* d_out;
+    double* h_out;     // pinned
+    double* d_stage;
+    size_t stage_elems;
+    cudaStream_t own_stream;
+    cudaStream_t stream;
+    int fused, tile_y, zchunk, ktiming;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_first, ev_last;
+    std::string err;
+    int device;
+};
+
+static int ctx_err(pf_ctx* c, int code, const std::string& msg)
+{
+    if (c) c->err = msg;
+    set_global_err(code, msg);
+    return code;
+}
+
+static int cuda_check(pf_ctx* c, cudaError_t e, const char* what)
+{
+    if (e == cudaSuccess) return PF_OK;
+    return ctx_err(c, PF_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call, what)                                  \
+    do {                                                \
+        int rc_ = cuda_check(ctx, (call), what);        \
+        if (rc_ != PF_OK) return rc_;                   \
+    } while (0)
+
+static inline bool is64(const pf_ctx* c) { return c->prec == PF_FP64; }
+
+static void fill_desc(const pf_grid& g, const pf_params& p, const pf_derived& dv, int px, DomainDesc& d)
+{
+    std::memset(&d, 0, sizeof(d));
+    d.nx = g.nx; d.ny = g.ny; d.nz = g.nz;
+    d.px = px;
+    d.plane = (long long)px * g.ny;
+    d.dx = g.dx; d.dy = g.dy; d.dz = g.dz;
+    d.E0 = dv.E0; d.W0 = dv.W0; d.DE = p.DELTA_EPSLON;
+    d.K_aniso = 16.0 * dv.E0 * p.DELTA_EPSLON;       // phase_body.inc:49
+    d.AAA = dv.AAA;
+    d.Ke = (double)p.Ke;
+    d.D_liq = p.D_liq; d.D_sol = p.D_sol;
+    d.dt = dv.DELTA_T;
+    d.dH_cp = p.delta_H / p.Cp_s;                     // temp_body.inc:36, cp = cp_s
+    d.Ddt = p.D * dv.DELTA_T;                         // temp_body.inc:41
+    d.cxy = 0.25 / (g.dx * g.dy);
+    d.cyz = 0.25 / (g.dy * g.dz);
+    d.czx = 0.25 / (g.dz * g.dx);
+    d.dx2 = g.dx * g.dx; d.dy2 = g.dy * g.dy; d.dz2 = g.dz * g.dz;
+    d.InvDX = 1.0 / (g.dx * g.dx); d.InvDY = 1.0 / (g.dy * g.dy); d.InvDZ = 1.0 / (g.dz * g.dz);
+    d.hx = 0.5 / g.dx; d.hy = 0.5 / g.dy; d.hz = 0.5 / g.dz;
+    d.rdx2 = 1.0 / (g.dx * g.dx); d.rdy2 = 1.0 / (g.dy * g.dy); d.rdz2 = 1.0 / (g.dz * g.dz);
+    d.hq = p.h_quintico;
+    d.rt = p.ruido_tipo;
+    d.do_heat_lap = (p.D != 0.0) ? 1 : 0;
+}
+
+static StepArgs make_step_args(const pf_ctx* c, int it, double TP_heat, double TP, double M0)
+{
+    StepArgs s;
+    std::memset(&s, 0, sizeof(s));
+    double Cs, Cl;
+    equilibrium(c->p, TP, &Cs, &Cl);
+    s.it = it;
+    s.TP_heat = TP_heat;
+    s.TP = TP;
+    s.M0dt = M0 * c->dv.DELTA_T;
+    s.RTV = c->p.R * TP / c->p.Vm;
+    s.omCs = 1.0 - Cs;
+    s.omCl = 1.0 - Cl;
+    return s;
+}
+
+static int validate(const pf_grid* g, const pf_params* p, int precision, std::string& why)
+{
+    if (!g || !p) { why = "null grid or params"; return PF_E_ARG; }
+    if (g->nx < 5 || g->ny < 5 || g->nz < 5) { why = "every grid dimension must be >= 5"; return PF_E_ARG; }
+    if (!(g->dx > 0) || !(g->dy > 0) || !(g->dz > 0)) { why = "grid spacings must be > 0"; return PF_E_ARG; }
+    if (precision != PF_FP64 && precision != PF_FP32) { why = "precision must be 64 or 32"; return PF_E_ARG; }
+    if (!(p->D_liq > 0) || !(p->Cp_s != 0) || !(p->Me != 0) || !(p->Vm != 0)) { why = "D_liq, Cp_s, Me, Vm must be nonzero"; return PF_E_ARG; }
+    if (p->n_varreduras < 1) { why = "n_varreduras must be >= 1"; return PF_E_ARG; }
+    if (p->h_quintico != 0 && p->h_quintico != 1) { why = "h_quintico must be 0 or 1"; return PF_E_ARG; }
+    if (p->ruido_tipo < 0 || p->ruido_tipo > 2) { why = "ruido_tipo must be 0, 1 or 2"; return PF_E_ARG; }
+    if (p->bc != PF_BC_REFERENCE) { why = "only the reference boundary treatment is available"; return PF_E_ARG; }
+    return PF_OK;
+}
+
+static size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+static int pitch_of(int nx) { return (int)round_up((size_t)nx, 32); }
+
+extern "C" {
+
+int pf_version(void) { return PF3D_VERSION; }
+
+const char* pf_last_error(const pf_ctx* ctx)
+{
+    if (ctx) return ctx->err.c_str();
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    return g_err.c_str();
+}
+
+long long pf_ctx_bytes(const pf_grid* g, int precision)
+{
+    if (!g || g->nx < 1 || g->ny < 1 || g->nz < 1) return -1;
+    size_t es = (precision == PF_FP32) ? 4 : 8;
+    size_t fb = round_up((size_t)pitch_of(g->nx) * g->ny * g->nz * es + 64, 256);
+    return (long long)(7 * fb);
+}
+
+int pf_create(const pf_grid* g, const pf_params* p, int precision, pf_ctx** out)
+{
+    if (!out) return set_global_err(PF_E_ARG, "out is null");
+    *out = nullptr;
+    std::string why;
+    int rc = validate(g, p, precision, why);
+    if (rc != PF_OK) return set_global_err(rc, why);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return set_global_err(PF_E_NODEV, "no CUDA device visible");
+    }
+    pf_ctx* ctx = new pf_ctx();
+    ctx->g = *g;
+    ctx->p = *p;
+    ctx->prec = precision;
+    ctx->es = (precision == PF_FP32) ? 4 : 8;
+    setup_derived(*g, *p, ctx->dv);
+    ctx->st.it = 0;
+    ctx->st.TP = initial_tp(*p);
+    ctx->st.M0 = p->M0;
+    ctx->st.time = 0.0f;
+    equilibrium(*p, ctx->st.TP, &ctx->st.Cs_eq, &ctx->st.Cl_eq);
+    const int px = pitch_of(g->nx);
+    fill_desc(*g, *p, ctx->dv, px, ctx->dd);
+    ctx->fused = 1;
+    ctx->tile_y = 8;
+    ctx->zchunk = 64;
+    ctx->ktiming = 0;
+    cudaGetDevice(&ctx->device);
+    // one allocation: 7 fields + diagnostics partials
+    ctx->field_bytes = round_up((size_t)px * g->ny * g->nz * ctx->es + 64, 256);
+    ctx->nblk = 592;
+    size_t total = 7 * ctx->field_bytes + (size_t)ctx->nblk * 8 * sizeof(double) + 8 * sizeof(double);
+    cudaError_t e = cudaMalloc(&ctx->base, total);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        delete ctx;
+        return set_global_err(PF_E_NOMEM, std::string("cudaMalloc of ") + std::to_string(total) + " bytes: " + cudaGetErrorString(e));
+    }
+    for (int f = 0; f < 7; ++f) ctx->fld[f] = (char*)ctx->base + (size_t)f * ctx->field_bytes;
+    ctx->d_part = (double*)((char*)ctx->base + 7 * ctx->field_bytes);
+    ctx->d_out = ctx->d_part + (size_t)ctx->nblk * 8;
+    if ((e = cudaMemset(ctx->base, 0, total)) != cudaSuccess ||
+        (e = cudaMallocHost(&ctx->h_out, 8 * sizeof(double))) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        cudaFree(ctx->base);
+        delete ctx;
+        return set_global_err(PF_E_CUDA, std::string("context set-up: ") + cudaGetErrorString(e));
+    }
+    ctx->stream = ctx->own_stream;
+    *out = ctx;
+    return PF_OK;
+}
+
+static void drop_events(pf_ctx* ctx)
+{
+    for (auto& pr : ctx->ev_first) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+    for (auto& pr : ctx->ev_last) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+    ctx->ev_first.clear();
+    ctx->ev_last.clear();
+}
+
+int pf_destroy(pf_ctx* ctx)
+{
+    if (!ctx) return PF_OK;
+    cudaStreamSynchronize(ctx->stream);
+    drop_events(ctx);
+    if (ctx->d_stage) cudaFree(ctx->d_stage);
+    cudaFree(ctx->base);
+    cudaFreeHost(ctx->h_out);
+    cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return PF_OK;
+}
+
+int pf_get_derived(const pf_ctx* ctx, pf_derived* out)
+{
+    if (!ctx || !out) return PF_E_ARG;
+    *out = ctx->dv;
+    return PF_OK;
+}
+
+int pf_get_state(const pf_ctx* ctx, pf_state* out)
+{
+    if (!ctx || !out) return PF_E_ARG;
+    *out = ctx->st;
+    return PF_OK;
+}
+
+int pf_set_state(pf_ctx* ctx, const pf_state* st)
+{
+    if (!ctx || !st) return PF_E_ARG;
+    ctx->st = *st;
+    return PF_OK;
+}
+
+int pf_sync(pf_ctx* ctx)
+{
+    if (!ctx) return PF_E_ARG;
+    CK(cudaStreamSynchronize(ctx->stream), "pf_sync");
+    return PF_OK;
+}
+
+int pf_set_stream(pf_ctx* ctx, void* stream)
+{
+    if (!ctx) return PF_E_ARG;
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return PF_OK;
+}
+
+int pf_set_option(pf_ctx* ctx, int opt, int value)
+{
+    if (!ctx) return PF_E_ARG;
+    switch (opt) {
+    case PF_OPT_FUSED: ctx->fused = value ? 1 : 0; return PF_OK;
+    case PF_OPT_TILE_Y:
+        if (value != 4 && value != 8 && value != 16) return ctx_err(ctx, PF_E_ARG, "tile_y must be 4, 8 or 16");
+        ctx->tile_y = value;
+        return PF_OK;
+    case PF_OPT_ZCHUNK:
+        if (value < 0) return ctx_err(ctx, PF_E_ARG, "zchunk must be >= 0");
+        ctx->zchunk = value;
+        return PF_OK;
+    case PF_OPT_KTIMING: ctx->ktiming = value ? 1 : 0; return PF_OK;
+    }
+    return ctx_err(ctx, PF_E_ARG, "unknown option");
+}
+
+int pf_get_option(const pf_ctx* ctx, int opt, int* value)
+{
+    if (!ctx || !value) return PF_E_ARG;
+    switch (opt) {
+    case PF_OPT_FUSED: *value = ctx->fused; return PF_OK;
+    case PF_OPT_TILE_Y: *value = ctx->tile_y; return PF_OK;
+    case PF_OPT_ZCHUNK: *value = ctx->zchunk; return PF_OK;
+    case PF_OPT_KTIMING: *value = ctx->ktiming; return PF_OK;
+    }
+    return PF_E_ARG;
+}
+
+// ---- data residency ----
+
+static int ensure_stage(pf_ctx* ctx)
+{
+    if (ctx->d_stage) return PF_OK;
+    size_t plane = (size_t)ctx->g.nx * ctx->g.ny;
+    size_t want = (size_t)1 << 24;  // 16 Mi doubles = 128 MiB
+    if (want < plane) want = plane;
+    ctx->stage_elems = want;
+    CK(cudaMalloc(&ctx->d_stage, want * sizeof(double)), "staging buffer");
+    return PF_OK;
+}
+
+int pf_upload(pf_ctx* ctx, int field, const double* host)
+{
+    if (!ctx || !host || field < 0 || field > 6) return ctx_err(ctx, PF_E_ARG, "pf_upload: bad argument");
+    const pf_grid& g = ctx->g;
+    if (is64(ctx)) {
+        CK(cudaMemcpy2DAsync(ctx->fld[field], (size_t)ctx->dd.px * 8, host, (size_t)g.nx * 8, (size_t)g.nx * 8,
+                             (size_t)g.ny * g.nz, cudaMemcpyHostToDevice, ctx->stream),
+           "pf_upload copy");
+    } else {
+        int rc = ensure_stage(ctx);
+        if (rc) return rc;
+        size_t plane = (size_t)g.nx * g.ny;
+        long long zper = (long long)(ctx->stage_elems / plane);
+        for (long long z0 = 0; z0 < g.nz; z0 += zper) {
+            long long nzc = std::min<long long>(zper, g.nz - z0);
+            CK(cudaMemcpyAsync(ctx->d_stage, host + z0 * plane, nzc * plane * sizeof(double), cudaMemcpyHostToDevice,
+                               ctx->stream),
+               "pf_upload copy");
+            CK(launch_convert_in<float>(ctx->dd, ctx->d_stage, ctx->fld[field], z0, nzc, ctx->stream), "pf_upload convert");
+        }
+    }
+    CK(cudaStreamSynchronize(ctx->stream), "pf_upload sync");
+    return PF_OK;
+}
+
+int pf_download(pf_ctx* ctx, int field, double* host)
+{
+    if (!ctx || !host || field < 0 || field > 6) return ctx_err(ctx, PF_E_ARG, "pf_download: bad argument");
+    const pf_grid& g = ctx->g;
+    if (is64(ctx)) {
+        CK(cudaMemcpy2DAsync(host, (size_t)g.nx * 8, ctx->fld[field], (size_t)ctx->dd.px * 8, (size_t)g.nx * 8,
+                             (size_t)g.ny * g.nz, cudaMemcpyDeviceToHost, ctx->stream),
+           "pf_download copy");
+    } else {
+        int rc = ensure_stage(ctx);
+        if (rc) return rc;
+        size_t plane = (size_t)g.nx * g.ny;
+        long long zper = (long long)(ctx->stage_elems / plane);
+        for (long long z0 = 0; z0 < g.nz; z0 += zper) {
+            long long nzc = std::min<long long>(zper, g.nz - z0);
+            CK(launch_convert_out<float>(ctx->dd, ctx->fld[field], ctx->d_stage, z0, nzc, ctx->stream), "pf_download convert");
+            CK(cudaMemcpyAsync(host + z0 * plane, ctx->d_stage, nzc * plane * sizeof(double), cudaMemcpyDeviceToHost,
+                               ctx->stream),
+               "pf_download copy");
+        }
+    }
+    CK(cudaStreamSynchronize(ctx->stream), "pf_download sync");
+    return PF_OK;
+}
+
+int pf_probe(pf_ctx* ctx, int field, int i, int j, int k, double* value)
+{
+    if (!ctx || !value || field < 0 || field > 6) return ctx_err(ctx, PF_E_ARG, "pf_probe: bad argument");
+    if (i < 1 || i > ctx->g.nx || j < 1 || j > ctx->g.ny || k < 1 || k > ctx->g.nz)
+        return ctx_err(ctx, PF_E_ARG, "pf_probe: index out of range");
+    size_t off = (size_t)(i - 1) + (size_t)ctx->dd.px * ((size_t)(j - 1) + (size_t)ctx->g.ny * (size_t)(k - 1));
+    CK(cudaMemcpyAsync(ctx->h_out, (char*)ctx->fld[field] + off * ctx->es, ctx->es, cudaMemcpyDeviceToHost, ctx->stream),
+       "pf_probe copy");
+    CK(cudaStreamSynchronize(ctx->stream), "pf_probe sync");
+    if (is64(ctx)) *value = ctx->h_out[0];
+    else { float f; std::memcpy(&f, ctx->h_out, 4); *value = (double)f; }
+    return PF_OK;
+}
+
+// ---- per-subroutine entry points ----
+
+static Fields fields_of(const pf_ctx* ctx)
+{
+    Fields f;
+    f.phi_old = ctx->fld[PF_PHASE_OLD];
+    f.phi_new = ctx->fld[PF_PHASE_NEW];
+    f.c_old = ctx->fld[PF_CONC_OLD];
+    f.c_new = ctx->fld[PF_CONC_NEW];
+    f.T_old = ctx->fld[PF_TOLD];
+    f.T_new = ctx->fld[PF_TNEW];
+    f.dpp = ctx->fld[PF_DPP];
+    f.phi_mid = nullptr;
+    return f;
+}
+
+int pf_temperatura(pf_ctx* ctx, double TP)
+{
+    if (!ctx) return PF_E_ARG;
+    StepArgs s = make_step_args(ctx, ctx->st.it, TP, TP, ctx->st.M0);
+    Fields f = fields_of(ctx);
+    CK(is64(ctx) ? launch_heat<double>(ctx->dd, s, f, ctx->stream) : launch_heat<float>(ctx->dd, s, f, ctx->stream),
+       "temperatura");
+    return PF_OK;
+}
+
+int pf_equacao_campo_fase(pf_ctx* ctx, int it, double TP, double M0, double* Cs_eq, double* Cl_eq)
+{
+    if (!ctx) return PF_E_ARG;
+    StepArgs s = make_step_args(ctx, it, TP, TP, M0);
+    double Cs, Cl;
+    equilibrium(ctx->p, TP, &Cs, &Cl);
+    ctx->st.Cs_eq = Cs;
+    ctx->st.Cl_eq = Cl;
+    if (Cs_eq) *Cs_eq = Cs;
+    if (Cl_eq) *Cl_eq = Cl;
+    Fields f = fields_of(ctx);
+    CK(is64(ctx) ? launch_phase<double>(ctx->dd, s, f.phi_old, f.c_old, f.phi_new, f.dpp, ctx->stream)
+                 : launch_phase<float>(ctx->dd, s, f.phi_old, f.c_old, f.phi_new, f.dpp, ctx->stream),
+       "equacao_campo_fase");
+    return PF_OK;
+}
+
+int pf_copy_phase_new_to_old(pf_ctx* ctx)
+{
+    if (!ctx) return PF_E_ARG;
+    CK(cudaMemcpyAsync(ctx->fld[PF_PHASE_OLD], ctx->fld[PF_PHASE_NEW], ctx->field_bytes, cudaMemcpyDeviceToDevice,
+                       ctx->stream),
+       "copy phase new->old");
+    return PF_OK;
+}
+
+int pf_concentracao_soluto(pf_ctx* ctx)
+{
+    if (!ctx) return PF_E_ARG;
+    StepArgs s = make_step_args(ctx, ctx->st.it, ctx->st.TP, ctx->st.TP, ctx->st.M0);
+    Fields f = fields_of(ctx);
+    if (is64(ctx)) {
+        CK(launch_solute<double>(ctx->dd, s, f.phi_old, f.c_old, f.c_new, ctx->stream), "concentracao_soluto");
+        CK(launch_copy_inner<double>(ctx->dd, f.c_new, f.c_old, ctx->stream), "concentracao_soluto old=new");
+    } else {
+        CK(launch_solute<float>(ctx->dd, s, f.phi_old, f.c_old, f.c_new, ctx->stream), "concentracao_soluto");
+        CK(launch_copy_inner<float>(ctx->dd, f.c_new, f.c_old, ctx->stream), "concentracao_soluto old=new");
+    }
+    return PF_OK;
+}
+
+int pf_auxiliar(const pf_ctx* ctx, double TP, double Cs_eq, double Cl_eq, double* M0)
+{
+    if (!ctx || !M0) return PF_E_ARG;
+    return pf_auxiliar_scalar(&ctx->p, ctx->dv.E0, ctx->dv.W0, TP, Cs_eq, Cl_eq, M0);
+}
+
+static int run_diag(pf_ctx* ctx, const void* phi, const void* c, double out[5])
+{
+    CK(is64(ctx) ? launch_diag<double>(ctx->dd, phi, c, ctx->d_part, ctx->nblk, ctx->d_out, ctx->stream)
+                 : launch_diag<float>(ctx->dd, phi, c, ctx->d_part, ctx->nblk, ctx->d_out, ctx->stream),
+       "diagnosticos");
+    CK(cudaMemcpyAsync(ctx->h_out, ctx->d_out, 5 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "diag copy");
+    CK(cudaStreamSynchronize(ctx->stream), "diag sync");
+    std::memcpy(out, ctx->h_out, 5 * sizeof(double));
+    return PF_OK;
+}
+
+int pf_diagnosticos(pf_ctx* ctx, double out[5])
+{
+    if (!ctx || !out) return PF_E_ARG;
+    return run_diag(ctx, ctx->fld[PF_PHASE_NEW], ctx->fld[PF_CONC_NEW], out);
+}
+
+int pf_swap(pf_ctx* ctx)
+{
+    if (!ctx) return PF_E_ARG;
+    std::swap(ctx->fld[PF_PHASE_OLD], ctx->fld[PF_PHASE_NEW]);
+    std::swap(ctx->fld[PF_TOLD], ctx->fld[PF_TNEW]);
+    std::swap(ctx->fld[PF_CONC_OLD], ctx->fld[PF_CONC_NEW]);
+    return PF_OK;
+}
+
+// ---- fused step ----
+
+static cudaEvent_t new_event()
+{
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+static int one_step(pf_ctx* ctx)
+{
+    const pf_params& p = ctx->p;
+    const int it = ctx->st.it + 1;
+    const double dt = ctx->dv.DELTA_T;
+    ctx->st.time = (float)(dt + (double)ctx->st.time);          // principal.f90:96 (REAL(4) time)
+    const double TP_heat = ctx->st.TP;                          // temperatura sees the previous TP
+    const double TP = step_tp(p, dt, it, ctx->st.TP);           // principal.f90:104
+    const StepArgs s = make_step_args(ctx, it, TP_heat, TP, ctx->st.M0);
+    const int nsw = p.n_varreduras;
+    void* A = ctx->fld[PF_PHASE_OLD];
+    void* B = ctx->fld[PF_PHASE_NEW];
+    Fields f = fields_of(ctx);
+    void* final_phi;
+    void* other_phi;
+    if (ctx->fused) {
+        if (nsw == 1) {
+            f.phi_mid = B;
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            if (ctx->ktiming) { e0 = new_event(); e1 = new_event(); cudaEventRecord(e0, ctx->stream); }
+            CK(is64(ctx) ? launch_fused_first<double>(ctx->dd, s, f, true, ctx->tile_y, ctx->zchunk, ctx->stream)
+                         : launch_fused_first<float>(ctx->dd, s, f, true, ctx->tile_y, ctx->zchunk, ctx->stream),
+               "fused step (single sweep)");
+            if (ctx->ktiming) { cudaEventRecord(e1, ctx->stream); ctx->ev_first.push_back({e0, e1}); }
+            final_phi = B;
+            other_phi = A;
+        } else {
+            f.phi_mid = B;
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            if (ctx->ktiming) { e0 = new_event(); e1 = new_event(); cudaEventRecord(e0, ctx->stream); }
+            CK(is64(ctx) ? launch_fused_first<double>(ctx->dd, s, f, false, ctx->tile_y, ctx->zchunk, ctx->stream)
+                         : launch_fused_first<float>(ctx->dd, s, f, false, ctx->tile_y, ctx->zchunk, ctx->stream),
+               "fused heat + sweep 1");
+            if (ctx->ktiming) { cudaEventRecord(e1, ctx->stream); ctx->ev_first.push_back({e0, e1}); }
+            void* cur = B;   // phase after the sweeps so far
+            void* oth = A;   // free buffer
+            for (int sw = 2; sw <= nsw - 1; ++sw) {
+                CK(is64(ctx) ? launch_phase<double>(ctx->dd, s, cur, f.c_old, oth, f.dpp, ctx->stream)
+                             : launch_phase<float>(ctx->dd, s, cur, f.c_old, oth, f.dpp, ctx->stream),
+                   "middle sweep");
+                std::swap(cur, oth);
+            }
+            Fields f2 = f;
+            f2.phi_mid = cur;
+            f2.phi_new = oth;
+            if (ctx->ktiming) { e0 = new_event(); e1 = new_event(); cudaEventRecord(e0, ctx->stream); }
+            CK(is64(ctx) ? launch_fused_last<double>(ctx->dd, s, f2, ctx->tile_y, ctx->zchunk, ctx->stream)
+                         : launch_fused_last<float>(ctx->dd, s, f2, ctx->tile_y, ctx->zchunk, ctx->stream),
+               "fused last sweep + solute");
+            if (ctx->ktiming) { cudaEventRecord(e1, ctx->stream); ctx->ev_last.push_back({e0, e1}); }
+            final_phi = oth;
+            other_phi = cur;
+        }
+    } else {
+        // per-subroutine kernels in the reference's order
+        CK(is64(ctx) ? launch_heat<double>(ctx->dd, s, f, ctx->stream) : launch_heat<float>(ctx->dd, s, f, ctx->stream),
+           "temperatura");
+        void* in = A;
+        void* out = B;
+        for (int sw = 1; sw <= nsw; ++sw) {
+            if (sw > 1) std::swap(in, out);   // the copy new -> old, by exchange
+            CK(is64(ctx) ? launch_phase<double>(ctx->dd, s, in, f.c_old, out, f.dpp, ctx->stream)
+                         : launch_phase<float>(ctx->dd, s, in, f.c_old, out, f.dpp, ctx->stream),
+               "equacao_campo_fase");
+        }
+        CK(is64(ctx) ? launch_solute<double>(ctx->dd, s, in, f.c_old, f.c_new, ctx->stream)
+                     : launch_solute<float>(ctx->dd, s, in, f.c_old, f.c_new, ctx->stream),
+           "concentracao_soluto");
+        final_phi = out;
+        other_phi = in;
+    }
+    // swap (principal.f90:200-226) by exchanging buffers
+    ctx->fld[PF_PHASE_OLD] = final_phi;
+    ctx->fld[PF_PHASE_NEW] = other_phi;
+    std::swap(ctx->fld[PF_CONC_OLD], ctx->fld[PF_CONC_NEW]);
+    std::swap(ctx->fld[PF_TOLD], ctx->fld[PF_TNEW]);
+    // auxiliar (principal.f90:157): M0 for the next step
+    double Cs, Cl;
+    equilibrium(p, TP, &Cs, &Cl);
+    double M0n;
+    pf_auxiliar_scalar(&p, ctx->dv.E0, ctx->dv.W0, TP, Cs, Cl, &M0n);
+    ctx->st.M0 = M0n;
+    ctx->st.TP = TP;
+    ctx->st.Cs_eq = Cs;
+    ctx->st.Cl_eq = Cl;
+    ctx->st.it = it;
+    return PF_OK;
+}
+
+int pf_step(pf_ctx* ctx, int n_steps)
+{
+    if (!ctx || n_steps < 0) return ctx_err(ctx, PF_E_ARG, "pf_step: bad argument");
+    for (int n = 0; n < n_steps; ++n) {
+        int rc = one_step(ctx);
+        if (rc) return rc;
+    }
+    return PF_OK;
+}
+
+int pf_step_diag(pf_ctx* ctx, int n_steps, double out[5])
+{
+    int rc = pf_step(ctx, n_steps);
+    if (rc) return rc;
+    // after the exchange the final state sits in the "old" buffers
+    return run_diag(ctx, ctx->fld[PF_PHASE_OLD], ctx->fld[PF_CONC_OLD], out);
+}
+
+int pf_kernel_times(pf_ctx* ctx, long* n_first, double* ms_first, long* n_last, double* ms_last, int reset)
+{
+    if (!ctx) return PF_E_ARG;
+    CK(cudaStreamSynchronize(ctx->stream), "pf_kernel_times sync");
+    double a = 0, b = 0;
+    for (auto& pr : ctx->ev_first) { float ms = 0; cudaEventElapsedTime(&ms, pr.first, pr.second); a += ms; }
+    for (auto& pr : ctx->ev_last) { float ms = 0; cudaEventElapsedTime(&ms, pr.first, pr.second); b += ms; }
+    if (n_first) *n_first = (long)ctx->ev_first.size();
+    if (ms_first) *ms_first = a;
+    if (n_last) *n_last = (long)ctx->ev_last.size();
+    if (ms_last) *ms_last = b;
+    if (reset) drop_events(ctx);
+    return PF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,379 @@
+// pf3d_device.cuh -- device-side data model and per-cell arithmetic of the
+// coupled explicit phase-field step (ileaof/phase-field-project-3D).
+//
+// Two arithmetic forms share this header:
+//   double : the plain form.  Every operation follows the reference's Fortran
+//            statement order (left-to-right association, x**2 = x*x,
+//            x**4 = (x*x)*(x*x), divisions kept as IEEE divisions).  The
+//            translation unit that instantiates it is compiled with
+//            --fmad=false so no multiply-add is contracted, matching gfortran
+//            on x86-64.
+//   float  : storage and stencil arithmetic in FP32; the divisions by grid
+//            constants become multiplications by host-rounded reciprocals.
+//            Its error is stated against the FP64 form, not bit parity.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pf3d {
+
+// ---------------------------------------------------------------------------
+// Per-domain constants (set once) and per-step scalars.  All host-computed in
+// FP64 with the reference's expressions, so FP64 kernels see the same bits the
+// reference's loop-invariant scalars have.
+// ---------------------------------------------------------------------------
+struct DomainDesc {
+    int nx, ny, nz;      // cells
+    int px;              // row pitch in elements (>= nx)
+    long long plane;     // px * ny
+    double dx, dy, dz;
+    double E0, W0, DE, K_aniso;   // K_aniso = 16*E0*DELTA_EPSLON (phase_body.inc:49)
+    double AAA;                   // effective noise amplitude
+    double Ke, D_liq, D_sol, dt;
+    double dH_cp;                 // delta_H / cp_s (temp_body.inc:36)
+    double Ddt;                   // D*DELTA_T of temp_body.inc:41 (D = 0 in the reference)
+    double cxy, cyz, czx;         // 0.25/(dx*dy), 0.25/(dy*dz), 0.25/(dz*dx)
+    double dx2, dy2, dz2;         // dx**2 ...
+    double InvDX, InvDY, InvDZ;   // 1/(DX*DX) ... (concentracao_soluto.f90:9-11)
+    double fl_dE;                 // FP32 only: 0.5/dx, 0.5/dy, 0.5/dz packed below
+    double hx, hy, hz;            // 0.5/dx, 0.5/dy, 0.5/dz (FP32 gradients)
+    double rdx2, rdy2, rdz2;      // 1/dx^2 ... (FP32)
+    double dE_scale;              // 0.5*E0*E0*dx*dy*dz factor pieces (diagnostics)
+    int hq;                       // h_quintico
+    int rt;                       // ruido_tipo
+    int do_heat_lap;              // D != 0
+    int pad_;
+};
+
+struct StepArgs {
+    int it;              // noise step index (1-based step number)
+    int pad_;
+    double TP_heat;      // TP seen by temperatura (the previous step's TP)
+    double TP;           // TP of this step's sweeps
+    double M0dt;         // M0*DELTA_T (phase_body.inc:194)
+    double RTV;          // R*TP/Vm (phase_body.inc:174)
+    double omCs, omCl;   // 1-Cs_eq, 1-Cl_eq
+};
+
+// ---------------------------------------------------------------------------
+// Noise: variaveis.f90:73-111.  Integer hash of 1-based (i,j,k,it,salt).
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ uint64_t hash63(int i, int j, int k, int it, int salt)
+{
+    uint64_t h = (uint64_t)(int64_t)i * 2654435761ull + (uint64_t)(int64_t)j * 2246822519ull +
+                 (uint64_t)(int64_t)k * 3266489917ull + (uint64_t)(int64_t)it * 668265263ull +
+                 (uint64_t)(int64_t)salt * 374761393ull + 1ull;
+    h ^= h >> 33;
+    h *= 0xff51afd7ed558ccdull;
+    h ^= h >> 33;
+    h *= 0xc4ceb9fe1a85ec53ull;
+    h ^= h >> 33;
+    return h & 0x7fffffffffffffffull;
+}
+
+// pseudo_random as FP64: the 63-bit integer rounded to double, then divided
+// by real(MASK63,8) = 2^63 (exact).
+__host__ __device__ __forceinline__ double ran64(uint64_t m)
+{
+    return (double)(long long)m * 0x1p-63;
+}
+
+__device__ __forceinline__ double ruido_suave64(int i, int j, int k, int it)
+{
+    const int LR = 6, TR = 20;
+    int i0 = i / LR, j0 = j / LR, k0 = k / LR, tb = it / TR;
+    double fx = (double)(i % LR) / (double)LR;
+    double fy = (double)(j % LR) / (double)LR;
+    double fz = (double)(k % LR) / (double)LR;
+    double p000 = ran64(hash63(i0, j0, k0, tb, 3)), p100 = ran64(hash63(i0 + 1, j0, k0, tb, 3));
+    double p010 = ran64(hash63(i0, j0 + 1, k0, tb, 3)), p110 = ran64(hash63(i0 + 1, j0 + 1, k0, tb, 3));
+    double p001 = ran64(hash63(i0, j0, k0 + 1, tb, 3)), p101 = ran64(hash63(i0 + 1, j0, k0 + 1, tb, 3));
+    double p011 = ran64(hash63(i0, j0 + 1, k0 + 1, tb, 3)), p111 = ran64(hash63(i0 + 1, j0 + 1, k0 + 1, tb, 3));
+    double a = __dadd_rn(__dmul_rn(1.0 - fx, p000), __dmul_rn(fx, p100));
+    double b = __dadd_rn(__dmul_rn(1.0 - fx, p010), __dmul_rn(fx, p110));
+    double c = __dadd_rn(__dmul_rn(1.0 - fx, p001), __dmul_rn(fx, p101));
+    double d = __dadd_rn(__dmul_rn(1.0 - fx, p011), __dmul_rn(fx, p111));
+    double lo = __dadd_rn(__dmul_rn(1.0 - fy, a), __dmul_rn(fy, b));
+    double hi = __dadd_rn(__dmul_rn(1.0 - fy, c), __dmul_rn(fy, d));
+    return __dadd_rn(__dmul_rn(1.0 - fz, lo), __dmul_rn(fz, hi));
+}
+
+// The REAL(4) `ran` of phase_body.inc:181-185 (identical for both precisions).
+__device__ __forceinline__ float phase_ran(int rt, int i, int j, int k, int it)
+{
+    double r = (rt == 2) ? ruido_suave64(i, j, k, it) : ran64(hash63(i, j, k, it, 1));
+    return __double2float_rn(r);
+}
+
+// ---------------------------------------------------------------------------
+// Arithmetic policy: FP64 keeps IEEE division and log; FP32 uses fast forms.
+// ---------------------------------------------------------------------------
+template <typename T> struct Ar;
+template <> struct Ar<double> {
+    static __device__ __forceinline__ double div(double a, double b) { return a / b; }
+    static __device__ __forceinline__ double lg(double x) { return log(x); }
+    static __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
+};
+template <> struct Ar<float> {
+    static __device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
+    static __device__ __forceinline__ float lg(float x) { return logf(x); }
+    static __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+};
+
+// Loop-invariant constants converted to the stencil type once per block.
+template <typename T>
+struct KC {
+    T dx, dy, dz, E0, W0, DE, K, AAA, Ke, D_liq, D_sol, dt, dH_cp, Ddt;
+    T cxy, cyz, czx, dx2, dy2, dz2, InvDX, InvDY, InvDZ;
+    T hx, hy, hz, rdx2, rdy2, rdz2;
+    T TP, TP_heat, M0dt, RTV, omCs, omCl;
+    int hq, rt, it, lap;
+    __device__ __forceinline__ void load(const DomainDesc& d, const StepArgs& s)
+    {
+        dx = (T)d.dx; dy = (T)d.dy; dz = (T)d.dz;
+        E0 = (T)d.E0; W0 = (T)d.W0; DE = (T)d.DE; K = (T)d.K_aniso; AAA = (T)d.AAA;
+        Ke = (T)d.Ke; D_liq = (T)d.D_liq; D_sol = (T)d.D_sol; dt = (T)d.dt;
+        dH_cp = (T)d.dH_cp; Ddt = (T)d.Ddt;
+        cxy = (T)d.cxy; cyz = (T)d.cyz; czx = (T)d.czx;
+        dx2 = (T)d.dx2; dy2 = (T)d.dy2; dz2 = (T)d.dz2;
+        InvDX = (T)d.InvDX; InvDY = (T)d.InvDY; InvDZ = (T)d.InvDZ;
+        hx = (T)d.hx; hy = (T)d.hy; hz = (T)d.hz;
+        rdx2 = (T)d.rdx2; rdy2 = (T)d.rdy2; rdz2 = (T)d.rdz2;
+        TP = (T)s.TP; TP_heat = (T)s.TP_heat; M0dt = (T)s.M0dt; RTV = (T)s.RTV;
+        omCs = (T)s.omCs; omCl = (T)s.omCl;
+        hq = d.hq; rt = d.rt; it = s.it; lap = d.do_heat_lap;
+    }
+};
+
+// node-centred central gradient component: (a-b)*0.5d0/dx (phase_body.inc:55-122)
+template <typename T>
+__device__ __forceinline__ T grad(T a, T b, T d, T half_inv)
+{
+    if constexpr (sizeof(T) == 8) return (a - b) * (T)0.5 / d;
+    else return (a - b) * half_inv;
+}
+
+// Anisotropy quantities at one node from its gradient (phase_body.inc:59-64):
+// eps and the three cross coefficients exy, eyz, ezx.
+template <typename T>
+struct Node { T eps, exy, eyz, ezx; };
+
+template <typename T>
+__device__ __forceinline__ Node<T> aniso_node(T gx, T gy, T gz, const KC<T>& c)
+{
+    Node<T> n;
+    T gx2 = gx * gx, gy2 = gy * gy, gz2 = gz * gz;
+    T Q = gx2 + gy2 + gz2 + (T)1e-23;
+    T S4 = gx2 * gx2 + gy2 * gy2 + gz2 * gz2;
+    T Q2 = Q * Q;
+    if constexpr (sizeof(T) == 8) {
+        n.eps = c.E0 * ((T)1 + c.DE * ((T)4 * S4 / Q2 - (T)3));
+        T Ke_ = c.K * n.eps;
+        n.exy = Ke_ * gx * gy * (gx2 - gy2) / Q2;
+        n.eyz = Ke_ * gy * gz * (gy2 - gz2) / Q2;
+        n.ezx = Ke_ * gz * gx * (gz2 - gx2) / Q2;
+    } else {
+        T rq = Ar<T>::rcp(Q2);
+        n.eps = c.E0 * ((T)1 + c.DE * ((T)4 * S4 * rq - (T)3));
+        T Ke_ = c.K * n.eps * rq;
+        n.exy = Ke_ * gx * gy * (gx2 - gy2);
+        n.eyz = Ke_ * gy * gz * (gy2 - gz2);
+        n.ezx = Ke_ * gz * gx * (gz2 - gx2);
+    }
+    return n;
+}
+
+// The 19 phase values of phase_body.inc:14-41.
+template <typename T>
+struct Nbr {
+    T PP, PN, PS, PE, PW, PT, PB;
+    T PNE, PSE, PNW, PSW, PNT, PNB, PST, PSB, PET, PEB, PWT, PWB;
+};
+
+// phase_body.inc:133-198 given the stencil values and the six node
+// quantities.  Returns PPNEW (unclamped).
+template <typename T>
+__device__ __forceinline__ T phase_ppnew(const Nbr<T>& p, const Node<T>& E, const Node<T>& W, const Node<T>& N,
+                                          const Node<T>& S, const Node<T>& Tt, const Node<T>& B, T CPP,
+                                          float ran, const KC<T>& c)
+{
+    const T PP = p.PP;
+    T AA, Cxy, Cyz, Czx;
+    if constexpr (sizeof(T) == 8) {
+        AA = (E.eps * E.eps * (p.PE - PP) + W.eps * W.eps * (p.PW - PP)) / c.dx2 +
+             (N.eps * N.eps * (p.PN - PP) + S.eps * S.eps * (p.PS - PP)) / c.dy2 +
+             (Tt.eps * Tt.eps * (p.PT - PP) + B.eps * B.eps * (p.PB - PP)) / c.dz2;
+        Cxy = c.cxy * (p.PNE * (-N.exy - (-E.exy)) + p.PSE * (-E.exy - (-S.exy)) + p.PNW * (-W.exy - (-N.exy)) +
+                       p.PSW * (-S.exy - (-W.exy))) +
+              p.PN * c.cxy * (-W.exy - (-E.exy)) + p.PS * c.cxy * (-E.exy - (-W.exy)) +
+              p.PE * c.cxy * (-N.exy - (-S.exy)) + p.PW * c.cxy * (-S.exy - (-N.exy));
+        Cyz = c.cyz * (p.PNT * (-Tt.eyz - (-N.eyz)) + p.PNB * (-N.eyz - (-B.eyz)) + p.PST * (-S.eyz - (-Tt.eyz)) +
+                       p.PSB * (-B.eyz - (-S.eyz))) +
+              p.PT * c.cyz * (-S.eyz - (-N.eyz)) + p.PB * c.cyz * (-N.eyz - (-S.eyz)) +
+              p.PN * c.cyz * (-Tt.eyz - (-B.eyz)) + p.PS * c.cyz * (-B.eyz - (-Tt.eyz));
+        Czx = c.czx * (p.PET * (-E.ezx - (-Tt.ezx)) + p.PWT * (-Tt.ezx - (-W.ezx)) + p.PEB * (-B.ezx - (-E.ezx)) +
+                       p.PWB * (-W.ezx - (-B.ezx))) +
+              p.PE * c.czx * (-B.ezx - (-Tt.ezx)) + p.PW * c.czx * (-Tt.ezx - (-B.ezx)) +
+              p.PT * c.czx * (-E.ezx - (-W.ezx)) + p.PB * c.czx * (-W.ezx - (-E.ezx));
+    } else {
+        AA = (E.eps * E.eps * (p.PE - PP) + W.eps * W.eps * (p.PW - PP)) * c.rdx2 +
+             (N.eps * N.eps * (p.PN - PP) + S.eps * S.eps * (p.PS - PP)) * c.rdy2 +
+             (Tt.eps * Tt.eps * (p.PT - PP) + B.eps * B.eps * (p.PB - PP)) * c.rdz2;
+        Cxy = c.cxy * (p.PNE * (E.exy - N.exy) + p.PSE * (S.exy - E.exy) + p.PNW * (N.exy - W.exy) +
+                       p.PSW * (W.exy - S.exy) + p.PN * (E.exy - W.exy) + p.PS * (W.exy - E.exy) +
+                       p.PE * (S.exy - N.exy) + p.PW * (N.exy - S.exy));
+        Cyz = c.cyz * (p.PNT * (N.eyz - Tt.eyz) + p.PNB * (B.eyz - N.eyz) + p.PST * (Tt.eyz - S.eyz) +
+                       p.PSB * (S.eyz - B.eyz) + p.PT * (N.eyz - S.eyz) + p.PB * (S.eyz - N.eyz) +
+                       p.PN * (B.eyz - Tt.eyz) + p.PS * (Tt.eyz - B.eyz));
+        Czx = c.czx * (p.PET * (Tt.ezx - E.ezx) + p.PWT * (W.ezx - Tt.ezx) + p.PEB * (E.ezx - B.ezx) +
+                       p.PWB * (B.ezx - W.ezx) + p.PE * (Tt.ezx - B.ezx) + p.PW * (B.ezx - Tt.ezx) +
+                       p.PT * (W.ezx - E.ezx) + p.PB * (E.ezx - W.ezx));
+    }
+    AA = AA + Cxy + Cyz + Czx;
+
+    const T one = (T)1, two = (T)2;
+    T g_linha = two * PP * (one - PP) * (one - PP) - two * PP * PP * (one - PP);
+    T h_linha, h;
+    if (c.hq == 1) {
+        h_linha = (T)30 * PP * PP * (one - PP) * (one - PP);
+        h = PP * PP * PP * ((T)10 - (T)15 * PP + (T)6 * PP * PP);
+    } else {
+        h_linha = two * PP * ((T)3 - two * PP) - two * PP * PP;
+        h = PP * PP * ((T)3 - two * PP);
+    }
+    T den = c.Ke * h + (one - h);
+    T CLP, CSP;
+    if constexpr (sizeof(T) == 8) {
+        CLP = CPP / den;
+        CSP = c.Ke * CPP / den;
+    } else {
+        T rd = Ar<T>::rcp(den);
+        CLP = CPP * rd;
+        CSP = c.Ke * CPP * rd;
+    }
+    T GG = (-(c.W0 * g_linha)) +
+           c.RTV * h_linha * Ar<T>::lg(fabs(Ar<T>::div(c.omCs * (one - CLP), c.omCl * (one - CSP))));
+    T pp2 = PP * PP, q = one - PP;
+    T ruidos;
+    if (c.rt == 0)
+        ruidos = (T)ran * c.AAA * (T)16 * pp2 * (q * q);
+    else
+        ruidos = (two * (T)ran - one) * c.AAA * (T)16 * pp2 * (q * q);
+    return PP + c.M0dt * (AA + GG) + ruidos;
+}
+
+// dmax1(0, dmin1(1, x)) (phase_body.inc:198)
+template <typename T>
+__device__ __forceinline__ T clamp01(T x)
+{
+    T t = (x < (T)1) ? x : (T)1;
+    return (t > (T)0) ? t : (T)0;
+}
+
+// h(phi) as written in conc_body.inc:42-58 (note the quintic form differs
+// from phase_body.inc:161 in its association).
+template <typename T>
+__device__ __forceinline__ T h_conc(T P, int hq)
+{
+    if (hq == 1) return (P * P * P) * ((T)10 - ((T)15 * P) + ((T)6 * (P * P)));
+    return P * P * ((T)3 - (T)2 * P);
+}
+
+// Per-point solute quantities of conc_body.inc: CL, the Gamma bracket
+// (1-h)CL(1-CL)+h CS(1-CS), and mu = log(CL/(1-CL)).
+template <typename T>
+struct SolNode { T br, mu; };
+
+template <typename T>
+__device__ __forceinline__ SolNode<T> sol_node(T P, T C, const KC<T>& c)
+{
+    const T one = (T)1;
+    T h = h_conc(P, c.hq);
+    T den = (c.Ke * h) + (one - h);
+    T CS, CL;
+    if constexpr (sizeof(T) == 8) {
+        CS = (c.Ke * C) / den;
+        CL = C / den;
+    } else {
+        T rd = Ar<T>::rcp(den);
+        CS = c.Ke * C * rd;
+        CL = C * rd;
+    }
+    SolNode<T> n;
+    n.br = (one - h) * CL * (one - CL) + h * CS * (one - CS);
+    n.mu = Ar<T>::lg(Ar<T>::div(CL, one - CL));
+    return n;
+}
+
+// conc_body.inc:92-149 given the seven per-point quantities.
+template <typename T>
+__device__ __forceinline__ T conc_new(T PP, T CPP, const SolNode<T>& P, const SolNode<T>& E, const SolNode<T>& W,
+                                      const SolNode<T>& N, const SolNode<T>& S, const SolNode<T>& Tt,
+                                      const SolNode<T>& B, const KC<T>& c)
+{
+    const T Dc = (PP <= (T)0.95) ? c.D_liq : c.D_sol;
+    const T two = (T)2, one = (T)1;
+    T GP = Dc * P.br, GS = Dc * S.br, GN = Dc * N.br, GW = Dc * W.br, GE = Dc * E.br, GT = Dc * Tt.br, GB = Dc * B.br;
+    T iP = Ar<T>::rcp(GP);
+    T Gs = Ar<T>::div(two, iP + Ar<T>::rcp(GS));
+    T Gn = Ar<T>::div(two, Ar<T>::rcp(GN) + iP);
+    T Gw = Ar<T>::div(two, iP + Ar<T>::rcp(GW));
+    T Ge = Ar<T>::div(two, Ar<T>::rcp(GE) + iP);
+    T Gt = Ar<T>::div(two, Ar<T>::rcp(GT) + iP);
+    T Gb = Ar<T>::div(two, iP + Ar<T>::rcp(GB));
+    (void)one;
+    return (Ge * c.InvDX * (E.mu - P.mu) - Gw * c.InvDX * (P.mu - W.mu) + Gn * c.InvDY * (N.mu - P.mu) -
+            Gs * c.InvDY * (P.mu - S.mu) + Gt * c.InvDZ * (Tt.mu - P.mu) - Gb * c.InvDZ * (P.mu - B.mu)) *
+               c.dt +
+           CPP;
+}
+
+// temp_body.inc:31-41 at an interior cell.
+template <typename T>
+__device__ __forceinline__ T heat_new(T PP, T dpp, T TE, T TW, T TN, T TS, T TT, T TB, const KC<T>& c)
+{
+    T h_linha;
+    if (c.hq == 1)
+        h_linha = (T)30 * PP * PP * ((T)1 - PP) * ((T)1 - PP);
+    else
+        h_linha = (T)2 * PP * ((T)3 - (T)2 * PP) - (T)2 * PP * PP;
+    T FONTE = c.dH_cp * h_linha * dpp;
+    if (c.lap) {
+        T TP = c.TP_heat;
+        T lap;
+        if constexpr (sizeof(T) == 8)
+            lap = ((TE - (T)2 * TP + TW) / c.dx2) + ((TN - (T)2 * TP + TS) / c.dy2) + ((TT - (T)2 * TP + TB) / c.dz2);
+        else
+            lap = ((TE - (T)2 * TP + TW) * c.rdx2) + ((TN - (T)2 * TP + TS) * c.rdy2) + ((TT - (T)2 * TP + TB) * c.rdz2);
+        return c.Ddt * lap + FONTE + TP;
+    }
+    // D = 0: D*DELTA_T*(finite) is a signed zero and drops out exactly.
+    return FONTE + c.TP_heat;
+}
+
+// ---------------------------------------------------------------------------
+// Boundary decoration in closed form (0-based indices).
+//   phase (equacao_campo_fase.f90:151-167, sequential in-place plane copies
+//   y, x, z): phi_new(x,y,z) = U(f(x), f(y), f(z)) with f(0)=1, f(1)=2,
+//   f(N-1)=N-2, f(N-2)=N-3, identity elsewhere (valid for N >= 5).
+//   A source cell therefore writes its value to every x' with f(x') = x.
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ int fmap(int x, int n)
+{
+    if (x == 0) return 1;
+    if (x == 1) return 2;
+    if (x == n - 1) return n - 2;
+    if (x == n - 2) return n - 3;
+    return x;
+}
+
+// preimages of a under fmap, written to out[]; returns the count (0..3)
+__host__ __device__ __forceinline__ int fpre(int a, int n, int out[3])
+{
+    int m = 0;
+    for (int x = a - 1; x <= a + 1; ++x)
+        if (x >= 0 && x < n && fmap(x, n) == a) out[m++] = x;
+    return m;
+}
+
+}  // namespace pf3d

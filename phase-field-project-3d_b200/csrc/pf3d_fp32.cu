@@ -1,0 +1,16 @@
+// pf3d_fp32.cu -- FP32 instantiation of every kernel (fields and stencils in FP32;
+// diagnostics still accumulate in FP64).  Multiply-adds may be contracted.
+#include "pf3d_simple.cuh"
+#include "pf3d_fused.cuh"
+
+namespace pf3d {
+template cudaError_t launch_heat<float>(const DomainDesc&, const StepArgs&, const Fields&, cudaStream_t);
+template cudaError_t launch_phase<float>(const DomainDesc&, const StepArgs&, const void*, const void*, void*, void*, cudaStream_t);
+template cudaError_t launch_solute<float>(const DomainDesc&, const StepArgs&, const void*, const void*, void*, cudaStream_t);
+template cudaError_t launch_copy_inner<float>(const DomainDesc&, const void*, void*, cudaStream_t);
+template cudaError_t launch_fused_first<float>(const DomainDesc&, const StepArgs&, const Fields&, bool, int, int, cudaStream_t);
+template cudaError_t launch_fused_last<float>(const DomainDesc&, const StepArgs&, const Fields&, int, int, cudaStream_t);
+template cudaError_t launch_diag<float>(const DomainDesc&, const void*, const void*, double*, int, double*, cudaStream_t);
+template cudaError_t launch_convert_in<float>(const DomainDesc&, const double*, void*, long long, long long, cudaStream_t);
+template cudaError_t launch_convert_out<float>(const DomainDesc&, const void*, double*, long long, long long, cudaStream_t);
+}  // namespace pf3d

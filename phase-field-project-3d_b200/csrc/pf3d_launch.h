@@ -1,0 +1,50 @@
+// pf3d_launch.h -- host-side launcher declarations.  The definitions are
+// templates in pf3d_kernels.cuh, instantiated for double in pf3d_fp64.cu
+// (built with --fmad=false) and for float in pf3d_fp32.cu.
+#pragma once
+#include <cuda_runtime.h>
+#include "pf3d_device.cuh"
+
+namespace pf3d {
+
+// Device pointers of one domain.  "old"/"new" follow the reference names.
+struct Fields {
+    void* phi_old;
+    void* phi_new;
+    void* c_old;
+    void* c_new;
+    void* T_old;
+    void* T_new;
+    void* dpp;
+    void* phi_mid;   // fused step: the sweep-1 phase field
+};
+
+// Per-subroutine kernels (one thread per cell, reference form).
+template <typename T> cudaError_t launch_heat(const DomainDesc& d, const StepArgs& s, const Fields& f, cudaStream_t st);
+template <typename T> cudaError_t launch_phase(const DomainDesc& d, const StepArgs& s, const void* phi_in,
+                                               const void* c_in, void* phi_out, void* dpp, cudaStream_t st);
+template <typename T> cudaError_t launch_solute(const DomainDesc& d, const StepArgs& s, const void* phi_in,
+                                                const void* c_in, void* c_out, cudaStream_t st);
+template <typename T> cudaError_t launch_copy_inner(const DomainDesc& d, const void* src, void* dst, cudaStream_t st);
+
+// Fused z-marching kernels.
+//   first  : temperatura + phase sweep 1 (phi_old -> phi_mid), or with
+//            solute as well when there is a single sweep
+//   last   : final phase sweep (phi_mid -> phi_new) + solute from phi_mid
+template <typename T> cudaError_t launch_fused_first(const DomainDesc& d, const StepArgs& s, const Fields& f,
+                                                     bool with_solute, int tile_y, int zchunk, cudaStream_t st);
+template <typename T> cudaError_t launch_fused_last(const DomainDesc& d, const StepArgs& s, const Fields& f,
+                                                    int tile_y, int zchunk, cudaStream_t st);
+
+// Diagnostics: block partials into part[nblk*8], final into out[5].
+template <typename T> cudaError_t launch_diag(const DomainDesc& d, const void* phi, const void* c, double* part,
+                                              int nblk, double* out, cudaStream_t st);
+
+// FP64 host array (Fortran order, nx*ny*nz) <-> pitched device field of T,
+// through a device staging buffer of doubles (FP32 contexts only).
+template <typename T> cudaError_t launch_convert_in(const DomainDesc& d, const double* stage, void* dst, long long z0,
+                                                    long long nz, cudaStream_t st);
+template <typename T> cudaError_t launch_convert_out(const DomainDesc& d, const void* src, double* stage, long long z0,
+                                                     long long nz, cudaStream_t st);
+
+}  // namespace pf3d

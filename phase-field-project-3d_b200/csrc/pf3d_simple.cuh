@@ -1,0 +1,323 @@
+// pf3d_simple.cuh -- one-thread-per-cell kernels behind the per-subroutine
+// entry points (pf_temperatura, pf_equacao_campo_fase, pf_concentracao_soluto,
+// pf_diagnosticos).  Each cell is computed in the reference form (six anisotropy
+// nodes per cell, seven solute points per cell); the boundary decoration is
+// applied in closed form by the thread that owns the source cell.
+#pragma once
+#include <cfloat>
+#include "pf3d_launch.h"
+
+namespace pf3d {
+
+__device__ __forceinline__ long long cell_off(const DomainDesc& d, int x, int y, int z)
+{
+    return (long long)x + (long long)y * d.px + (long long)z * d.plane;
+}
+
+// ---- temperatura.f90 (TNEW = TOLD; temp_body.inc on 2..N-1) ----
+template <typename T>
+__global__ void __launch_bounds__(256) k_heat(DomainDesc d, StepArgs s, const T* __restrict__ Told,
+                                              const T* __restrict__ phi, const T* __restrict__ dpp,
+                                              T* __restrict__ Tnew)
+{
+    int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    if (x >= d.nx || y >= d.ny) return;
+    long long id = cell_off(d, x, y, z);
+    bool inner = x >= 1 && x <= d.nx - 2 && y >= 1 && y <= d.ny - 2 && z >= 1 && z <= d.nz - 2;
+    if (!inner) { Tnew[id] = Told[id]; return; }
+    KC<T> c;
+    c.load(d, s);
+    T TE = 0, TW = 0, TN = 0, TS = 0, TT = 0, TB = 0;
+    if (c.lap) {
+        TE = Told[id + 1]; TW = Told[id - 1]; TN = Told[id + d.px]; TS = Told[id - d.px];
+        TT = Told[id + d.plane]; TB = Told[id - d.plane];
+    }
+    Tnew[id] = heat_new<T>(phi[id], dpp[id], TE, TW, TN, TS, TT, TB, c);
+}
+
+// ---- equacao_campo_fase.f90 (copy, phase_body.inc on 3..N-2, decoration) ----
+template <typename T>
+__global__ void __launch_bounds__(256) k_phase(DomainDesc d, StepArgs s, const T* __restrict__ po,
+                                               const T* __restrict__ co, T* __restrict__ pn, T* __restrict__ dpp)
+{
+    int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    if (x >= d.nx || y >= d.ny) return;
+    // only cells with every coordinate in [1, N-2] are decoration sources
+    if (x < 1 || x > d.nx - 2 || y < 1 || y > d.ny - 2 || z < 1 || z > d.nz - 2) return;
+    long long id = cell_off(d, x, y, z);
+    T U;
+    if (x >= 2 && x <= d.nx - 3 && y >= 2 && y <= d.ny - 3 && z >= 2 && z <= d.nz - 3) {
+        KC<T> c;
+        c.load(d, s);
+        const T* p = po + id;
+        const long long sy = d.px, sz = d.plane;
+        auto P = [&](int a, int b, int e) -> T { return p[a + b * sy + e * sz]; };
+        Nbr<T> nb;
+        nb.PP = P(0, 0, 0);
+        nb.PN = P(0, 1, 0); nb.PS = P(0, -1, 0); nb.PE = P(1, 0, 0); nb.PW = P(-1, 0, 0);
+        nb.PT = P(0, 0, 1); nb.PB = P(0, 0, -1);
+        nb.PNE = P(1, 1, 0); nb.PSE = P(1, -1, 0); nb.PNW = P(-1, 1, 0); nb.PSW = P(-1, -1, 0);
+        nb.PNT = P(0, 1, 1); nb.PNB = P(0, 1, -1); nb.PST = P(0, -1, 1); nb.PSB = P(0, -1, -1);
+        nb.PET = P(1, 0, 1); nb.PEB = P(1, 0, -1); nb.PWT = P(-1, 0, 1); nb.PWB = P(-1, 0, -1);
+        Node<T> E = aniso_node<T>(grad<T>(P(2, 0, 0), nb.PP, c.dx, c.hx), grad<T>(P(1, 1, 0), P(1, -1, 0), c.dy, c.hy),
+                                  grad<T>(P(1, 0, 1), P(1, 0, -1), c.dz, c.hz), c);
+        Node<T> W = aniso_node<T>(grad<T>(nb.PP, P(-2, 0, 0), c.dx, c.hx), grad<T>(P(-1, 1, 0), P(-1, -1, 0), c.dy, c.hy),
+                                  grad<T>(P(-1, 0, 1), P(-1, 0, -1), c.dz, c.hz), c);
+        Node<T> N = aniso_node<T>(grad<T>(P(1, 1, 0), P(-1, 1, 0), c.dx, c.hx), grad<T>(P(0, 2, 0), nb.PP, c.dy, c.hy),
+                                  grad<T>(P(0, 1, 1), P(0, 1, -1), c.dz, c.hz), c);
+        Node<T> S = aniso_node<T>(grad<T>(P(1, -1, 0), P(-1, -1, 0), c.dx, c.hx), grad<T>(nb.PP, P(0, -2, 0), c.dy, c.hy),
+                                  grad<T>(P(0, -1, 1), P(0, -1, -1), c.dz, c.hz), c);
+        Node<T> Tt = aniso_node<T>(grad<T>(P(1, 0, 1), P(-1, 0, 1), c.dx, c.hx), grad<T>(P(0, 1, 1), P(0, -1, 1), c.dy, c.hy),
+                                   grad<T>(P(0, 0, 2), nb.PP, c.dz, c.hz), c);
+        Node<T> B = aniso_node<T>(grad<T>(P(1, 0, -1), P(-1, 0, -1), c.dx, c.hx), grad<T>(P(0, 1, -1), P(0, -1, -1), c.dy, c.hy),
+                                  grad<T>(nb.PP, P(0, 0, -2), c.dz, c.hz), c);
+        float ran = phase_ran(c.rt, x + 1, y + 1, z + 1, c.it);
+        T ppn = phase_ppnew<T>(nb, E, W, N, S, Tt, B, co[id], ran, c);
+        dpp[id] = ppn - nb.PP;
+        U = clamp01(ppn);
+    } else {
+        U = po[id];
+    }
+    int xs[3], ys[3], zs[3];
+    int mx = fpre(x, d.nx, xs), my = fpre(y, d.ny, ys), mz = fpre(z, d.nz, zs);
+    for (int a = 0; a < mz; ++a)
+        for (int b = 0; b < my; ++b)
+            for (int e = 0; e < mx; ++e) pn[cell_off(d, xs[e], ys[b], zs[a])] = U;
+}
+
+// ---- concentracao_soluto.f90 (conc_body.inc on 2..N-1, decoration) ----
+template <typename T>
+__global__ void __launch_bounds__(256) k_solute(DomainDesc d, StepArgs s, const T* __restrict__ po,
+                                                const T* __restrict__ co, T* __restrict__ cn)
+{
+    int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    if (x >= d.nx || y >= d.ny) return;
+    long long id = cell_off(d, x, y, z);
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    bool xin = x >= 1 && x <= nx - 2, yin = y >= 1 && y <= ny - 2, zin = z >= 1 && z <= nz - 2;
+    bool inner = xin && yin && zin;
+    // only inner cells, or cells one plane from a wall, feed a write
+    bool feeds = inner || z == 1 || z == nz - 2 || (zin && (x == 1 || x == nx - 2));
+    if (!feeds) return;
+    T U;
+    if (inner) {
+        KC<T> c;
+        c.load(d, s);
+        const long long sy = d.px, sz = d.plane;
+        T PP = po[id];
+        SolNode<T> nP = sol_node<T>(PP, co[id], c);
+        SolNode<T> nE = sol_node<T>(po[id + 1], co[id + 1], c);
+        SolNode<T> nW = sol_node<T>(po[id - 1], co[id - 1], c);
+        SolNode<T> nN = sol_node<T>(po[id + sy], co[id + sy], c);
+        SolNode<T> nS = sol_node<T>(po[id - sy], co[id - sy], c);
+        SolNode<T> nT = sol_node<T>(po[id + sz], co[id + sz], c);
+        SolNode<T> nB = sol_node<T>(po[id - sz], co[id - sz], c);
+        U = conc_new<T>(PP, co[id], nP, nE, nW, nN, nS, nT, nB, c);
+        cn[id] = U;
+    } else {
+        U = co[id];
+    }
+    // last writer wins in the order y, x, z faces (concentracao_soluto.f90:119-124)
+    if (z == 1) cn[cell_off(d, x, y, 0)] = U;
+    if (z == nz - 2) cn[cell_off(d, x, y, nz - 1)] = U;
+    if (zin && x == 1) cn[cell_off(d, 0, y, z)] = U;
+    if (zin && x == nx - 2) cn[cell_off(d, nx - 1, y, z)] = U;
+    if (zin && xin && y == 1) cn[cell_off(d, x, 0, z)] = U;
+    if (zin && xin && y == ny - 2) cn[cell_off(d, x, ny - 1, z)] = U;
+}
+
+// conc_soluto_old = conc_soluto_new on 2..N-1 (the wall cells of
+// conc_soluto_old keep their values; concentracao_soluto.f90:116)
+template <typename T>
+__global__ void __launch_bounds__(256) k_copy_inner(DomainDesc d, const T* __restrict__ src, T* __restrict__ dst)
+{
+    int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    if (x < 1 || x > d.nx - 2 || y < 1 || y > d.ny - 2 || z < 1 || z > d.nz - 2) return;
+    long long id = cell_off(d, x, y, z);
+    dst[id] = src[id];
+}
+
+// ---- diagnosticos.f90 + diag_body.inc ----
+// FP64 accumulation with Neumaier compensation; max/min exact.
+struct KSum {
+    double s, c;
+    __device__ __forceinline__ void add(double v)
+    {
+        double t = s + v;
+        if (fabs(s) >= fabs(v)) c += (s - t) + v;
+        else c += (v - t) + s;
+        s = t;
+    }
+    __device__ __forceinline__ void merge(double os, double oc)
+    {
+        add(os);
+        c += oc;
+    }
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_diag(DomainDesc d, const T* __restrict__ pn, const T* __restrict__ cn,
+                                              double* __restrict__ part)
+{
+    const long long ncell = (long long)d.nx * d.ny * d.nz;
+    KSum l2{0, 0}, sol{0, 0}, fe{0, 0};
+    double mx = -DBL_MAX, mn = DBL_MAX;
+    const double dx = d.dx, dy = d.dy, dz = d.dz, E0 = d.E0, w0 = d.W0;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
+        int x = (int)(q % d.nx);
+        long long r = q / d.nx;
+        int y = (int)(r % d.ny);
+        int z = (int)(r / d.ny);
+        long long id = cell_off(d, x, y, z);
+        double phi = (double)pn[id];
+        l2.add(phi * phi);
+        mx = fmax(mx, phi);
+        mn = fmin(mn, phi);
+        sol.add((double)cn[id]);
+        double w_term = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(w0, phi), phi), 1.0 - phi), 1.0 - phi);
+        double grad2 = 0.0;
+        if (x > 0 && x < d.nx - 1 && y > 0 && y < d.ny - 1 && z > 0 && z < d.nz - 1) {
+            double gx = __dmul_rn((double)pn[id + 1] - (double)pn[id - 1], 0.5) / dx;
+            double gy = __dmul_rn((double)pn[id + d.px] - (double)pn[id - d.px], 0.5) / dy;
+            double gz = __dmul_rn((double)pn[id + d.plane] - (double)pn[id - d.plane], 0.5) / dz;
+            grad2 = __dadd_rn(__dadd_rn(__dmul_rn(gx, gx), __dmul_rn(gy, gy)), __dmul_rn(gz, gz));
+        }
+        double e = __dadd_rn(__dmul_rn(__dmul_rn(__dmul_rn(0.5, E0), E0), grad2), w_term);
+        fe.add(__dmul_rn(__dmul_rn(__dmul_rn(e, dx), dy), dz));
+    }
+    __shared__ double sh[8][8];
+    double v[8] = {l2.s, l2.c, mx, mn, sol.s, sol.c, fe.s, fe.c};
+    // warp reduction (fixed order, deterministic for a fixed launch shape)
+    for (int off = 16; off > 0; off >>= 1) {
+        double o[8];
+        for (int q = 0; q < 8; ++q) o[q] = __shfl_down_sync(0xffffffffu, v[q], off);
+        KSum a{v[0], v[1]}; a.merge(o[0], o[1]); v[0] = a.s; v[1] = a.c;
+        v[2] = fmax(v[2], o[2]); v[3] = fmin(v[3], o[3]);
+        KSum b{v[4], v[5]}; b.merge(o[4], o[5]); v[4] = b.s; v[5] = b.c;
+        KSum e{v[6], v[7]}; e.merge(o[6], o[7]); v[6] = e.s; v[7] = e.c;
+    }
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0)
+        for (int q = 0; q < 8; ++q) sh[w][q] = v[q];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int nw = blockDim.x >> 5;
+        for (int q = 0; q < 8; ++q) v[q] = sh[0][q];
+        for (int ww = 1; ww < nw; ++ww) {
+            KSum a{v[0], v[1]}; a.merge(sh[ww][0], sh[ww][1]); v[0] = a.s; v[1] = a.c;
+            v[2] = fmax(v[2], sh[ww][2]); v[3] = fmin(v[3], sh[ww][3]);
+            KSum b{v[4], v[5]}; b.merge(sh[ww][4], sh[ww][5]); v[4] = b.s; v[5] = b.c;
+            KSum e{v[6], v[7]}; e.merge(sh[ww][6], sh[ww][7]); v[6] = e.s; v[7] = e.c;
+        }
+        for (int q = 0; q < 8; ++q) part[(long long)blockIdx.x * 8 + q] = v[q];
+    }
+}
+
+template <typename T>  // templated only so each precision unit owns its copy
+__global__ void k_diag_final(const double* __restrict__ part, int nblk, double* __restrict__ out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    KSum l2{0, 0}, sol{0, 0}, fe{0, 0};
+    double mx = -DBL_MAX, mn = DBL_MAX;
+    for (int b = 0; b < nblk; ++b) {
+        const double* p = part + (long long)b * 8;
+        l2.merge(p[0], p[1]);
+        mx = fmax(mx, p[2]);
+        mn = fmin(mn, p[3]);
+        sol.merge(p[4], p[5]);
+        fe.merge(p[6], p[7]);
+    }
+    out[0] = sqrt(l2.s + l2.c);
+    out[1] = mx;
+    out[2] = mn;
+    out[3] = sol.s + sol.c;
+    out[4] = fe.s + fe.c;
+}
+
+// ---- host conversion staging (FP32 contexts) ----
+template <typename T>
+__global__ void k_convert_in(DomainDesc d, const double* __restrict__ stage, T* __restrict__ dst, long long z0, long long nzc)
+{
+    long long n = (long long)d.nx * d.ny * nzc;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        int x = (int)(q % d.nx);
+        long long r = q / d.nx;
+        int y = (int)(r % d.ny);
+        long long z = z0 + r / d.ny;
+        dst[x + (long long)y * d.px + z * d.plane] = (T)stage[q];
+    }
+}
+
+template <typename T>
+__global__ void k_convert_out(DomainDesc d, const T* __restrict__ src, double* __restrict__ stage, long long z0, long long nzc)
+{
+    long long n = (long long)d.nx * d.ny * nzc;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        int x = (int)(q % d.nx);
+        long long r = q / d.nx;
+        int y = (int)(r % d.ny);
+        long long z = z0 + r / d.ny;
+        stage[q] = (double)src[x + (long long)y * d.px + z * d.plane];
+    }
+}
+
+// ---- launchers ----
+inline dim3 cell_grid(const DomainDesc& d) { return dim3((d.nx + 31) / 32, (d.ny + 7) / 8, d.nz); }
+
+template <typename T>
+cudaError_t launch_heat(const DomainDesc& d, const StepArgs& s, const Fields& f, cudaStream_t st)
+{
+    k_heat<T><<<cell_grid(d), dim3(32, 8), 0, st>>>(d, s, (const T*)f.T_old, (const T*)f.phi_old, (const T*)f.dpp,
+                                                    (T*)f.T_new);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_phase(const DomainDesc& d, const StepArgs& s, const void* phi_in, const void* c_in, void* phi_out,
+                         void* dpp, cudaStream_t st)
+{
+    k_phase<T><<<cell_grid(d), dim3(32, 8), 0, st>>>(d, s, (const T*)phi_in, (const T*)c_in, (T*)phi_out, (T*)dpp);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_solute(const DomainDesc& d, const StepArgs& s, const void* phi_in, const void* c_in, void* c_out,
+                          cudaStream_t st)
+{
+    k_solute<T><<<cell_grid(d), dim3(32, 8), 0, st>>>(d, s, (const T*)phi_in, (const T*)c_in, (T*)c_out);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_copy_inner(const DomainDesc& d, const void* src, void* dst, cudaStream_t st)
+{
+    k_copy_inner<T><<<cell_grid(d), dim3(32, 8), 0, st>>>(d, (const T*)src, (T*)dst);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_diag(const DomainDesc& d, const void* phi, const void* c, double* part, int nblk, double* out,
+                        cudaStream_t st)
+{
+    k_diag<T><<<nblk, 256, 0, st>>>(d, (const T*)phi, (const T*)c, part);
+    k_diag_final<T><<<1, 32, 0, st>>>(part, nblk, out);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_convert_in(const DomainDesc& d, const double* stage, void* dst, long long z0, long long nzc,
+                              cudaStream_t st)
+{
+    k_convert_in<T><<<592, 256, 0, st>>>(d, stage, (T*)dst, z0, nzc);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_convert_out(const DomainDesc& d, const void* src, double* stage, long long z0, long long nzc,
+                               cudaStream_t st)
+{
+    k_convert_out<T><<<592, 256, 0, st>>>(d, (const T*)src, stage, z0, nzc);
+    return cudaGetLastError();
+}
+
+}  // namespace pf3d
