@@ -216,7 +216,9 @@ def main():
     prec = w.precision
     cells = w.cells
     st = init.initial_state(w.nx, w.ny, w.nz, w.n_bumps, w.seed + rank, p)
-    stream = torch.cuda.current_stream()
+    # a dedicated (non-legacy) stream: the library runs on it and the events see it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
 
     dom = pf3d.Domain(g, p, prec)
     dom.set_stream(stream.cuda_stream)

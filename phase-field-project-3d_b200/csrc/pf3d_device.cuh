@@ -367,13 +367,12 @@ __host__ __device__ __forceinline__ int fmap(int x, int n)
     return x;
 }
 
-// preimages of a under fmap, written to out[]; returns the count (0..3)
-__host__ __device__ __forceinline__ int fpre(int a, int n, int out[3])
+// Preimages of a source coordinate a in [1, N-2] under fmap: the contiguous
+// range [*lo, *hi] (one to three cells).
+__host__ __device__ __forceinline__ void fpre_range(int a, int n, int* lo, int* hi)
 {
-    int m = 0;
-    for (int x = a - 1; x <= a + 1; ++x)
-        if (x >= 0 && x < n && fmap(x, n) == a) out[m++] = x;
-    return m;
+    *lo = (a == 1) ? 0 : (a == 2) ? 1 : (a == n - 2) ? n - 1 : a;
+    *hi = (a == n - 2) ? n - 1 : (a == n - 3) ? n - 2 : (a == 1) ? 0 : a;
 }
 
 }  // namespace pf3d

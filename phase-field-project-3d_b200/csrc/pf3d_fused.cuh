@@ -46,7 +46,7 @@ struct FusedSmem {
 };
 
 template <typename T, int TY, bool HEAT, bool DPPW, bool SOL>
-__global__ void __launch_bounds__(32 * TY) k_fused(DomainDesc d, StepArgs s, const T* __restrict__ phi_in,
+__global__ void __launch_bounds__(32 * TY, (TY <= 8) ? 2 : 1) k_fused(DomainDesc d, StepArgs s, const T* __restrict__ phi_in,
                                                    const T* __restrict__ c_in, T* __restrict__ phi_out,
                                                    T* __restrict__ dpp, T* __restrict__ c_out,
                                                    const T* __restrict__ T_old, T* __restrict__ T_new, int zchunk)
@@ -140,9 +140,9 @@ __global__ void __launch_bounds__(32 * TY) k_fused(DomainDesc d, StepArgs s, con
     const int nlx = tx + 1, nly = ty + 1; // own cell in the node tile
     const bool xs_src = x >= 1 && x <= nx - 2, ys_src = y >= 1 && y <= ny - 2;
     const bool xs_int = x >= 2 && x <= nx - 3, ys_int = y >= 2 && y <= ny - 3;
-    int xpre[3], ypre[3];
-    const int mxp = own ? fpre(x, nx, xpre) : 0;
-    const int myp = own ? fpre(y, ny, ypre) : 0;
+    int xl = 0, xh = -1, yl = 0, yh = -1;
+    if (own && xs_src) fpre_range(x, nx, &xl, &xh);
+    if (own && ys_src) fpre_range(y, ny, &yl, &yh);
 
     for (int z = zb; z < ze; ++z) {
         node_plane(z + 1);
@@ -206,12 +206,12 @@ __global__ void __launch_bounds__(32 * TY) k_fused(DomainDesc d, StepArgs s, con
                 } else {
                     U = PPc;
                 }
-                int zpre[3];
-                const int mzp = fpre(z, nz, zpre);
-                for (int a = 0; a < mzp; ++a)
-                    for (int b = 0; b < myp; ++b)
-                        for (int e = 0; e < mxp; ++e)
-                            phi_out[(long long)xpre[e] + (long long)ypre[b] * px + (long long)zpre[a] * pl] = U;
+                int zl, zh;
+                fpre_range(z, nz, &zl, &zh);
+                for (int zz = zl; zz <= zh; ++zz)
+                    for (int yy = yl; yy <= yh; ++yy)
+                        for (int xx = xl; xx <= xh; ++xx)
+                            phi_out[(long long)xx + (long long)yy * px + (long long)zz * pl] = U;
             }
 
             // ---- solute ----

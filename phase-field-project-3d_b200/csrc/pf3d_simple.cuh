@@ -78,11 +78,13 @@ __global__ void __launch_bounds__(256) k_phase(DomainDesc d, StepArgs s, const T
     } else {
         U = po[id];
     }
-    int xs[3], ys[3], zs[3];
-    int mx = fpre(x, d.nx, xs), my = fpre(y, d.ny, ys), mz = fpre(z, d.nz, zs);
-    for (int a = 0; a < mz; ++a)
-        for (int b = 0; b < my; ++b)
-            for (int e = 0; e < mx; ++e) pn[cell_off(d, xs[e], ys[b], zs[a])] = U;
+    int xl, xh, yl, yh, zl, zh;
+    fpre_range(x, d.nx, &xl, &xh);
+    fpre_range(y, d.ny, &yl, &yh);
+    fpre_range(z, d.nz, &zl, &zh);
+    for (int zz = zl; zz <= zh; ++zz)
+        for (int yy = yl; yy <= yh; ++yy)
+            for (int xx = xl; xx <= xh; ++xx) pn[cell_off(d, xx, yy, zz)] = U;
 }
 
 // ---- concentracao_soluto.f90 (conc_body.inc on 2..N-1, decoration) ----

@@ -132,16 +132,50 @@ def test_fused_equals_per_subroutine_bitwise(gpu, tile_y, zchunk):
             assert np.array_equal(fa[k], fb[k]), k
 
 
+def exact_diagnostics(phi, c, dx, dy, dz, E0, w0):
+    """diag_body.inc evaluated per cell in the reference's order, summed with
+    math.fsum (exactly rounded) -- the reference's OpenMP reduction order is
+    unspecified, so its rounding is not a target."""
+    import math
+    nz, ny, nx = phi.shape
+    w_term = w0 * phi * phi * (1.0 - phi) * (1.0 - phi)
+    grad2 = np.zeros_like(phi)
+    gx = (phi[1:-1, 1:-1, 2:] - phi[1:-1, 1:-1, :-2]) * 0.5 / dx
+    gy = (phi[1:-1, 2:, 1:-1] - phi[1:-1, :-2, 1:-1]) * 0.5 / dy
+    gz = (phi[2:, 1:-1, 1:-1] - phi[:-2, 1:-1, 1:-1]) * 0.5 / dz
+    grad2[1:-1, 1:-1, 1:-1] = gx ** 2 + gy ** 2 + gz ** 2
+    fe = (0.5 * E0 * E0 * grad2 + w_term) * dx * dy * dz
+    return (math.sqrt(math.fsum((phi * phi).ravel())), float(phi.max()), float(phi.min()),
+            math.fsum(c.ravel()), math.fsum(fe.ravel()))
+
+
 def test_diagnosticos_match_oracle(gpu):
     g, p, st = c1_case()
     o = O.Oracle(g, p); o.load_state(st)
     o.step(3)
-    ref = o.diagnosticos()          # after the swap new == old in the oracle
+    sc = o.scalars()
+    fo = o.fields()
+    ref = exact_diagnostics(fo["phi"], fo["c"], g.dx, g.dy, g.dz, sc["E0"], sc["W0"])
+    naive = o.diagnosticos()        # serial sums (after the swap new == old)
     with pf3d.Domain(g, p) as d:
         d.load_state(st)
         out = d.step_diag(3)
+    for a, b, c in zip(out, ref, naive):
+        assert abs(a - b) <= 1e-12 * abs(b), (out, ref)
+        assert abs(c - b) <= 1e-9 * abs(b)      # the naive serial sum, for scale
+
+
+def test_diagnosticos_entry_point(gpu):
+    """pf_diagnosticos reads phase_field_new / conc_soluto_new, as the reference."""
+    g, p, st = small_case(30, 26, 34)
+    with pf3d.Domain(g, p) as d:
+        d.upload("phase_field_new", st["phi"])
+        d.upload("conc_soluto_new", st["c"])
+        out = d.diagnosticos()
+        dv = d.derived()
+    ref = exact_diagnostics(st["phi"], st["c"], g.dx, g.dy, g.dz, dv.E0, dv.W0)
     for a, b in zip(out, ref):
-        assert abs(a - b) <= 1e-12 * max(abs(b), 1e-300), (out, ref)
+        assert abs(a - b) <= 1e-12 * abs(b), (out, ref)
 
 
 @pytest.mark.slow
