@@ -185,6 +185,24 @@ int pf_diagnosticos(pf_ctx* ctx, double out[5]);
    them in between).                                                        */
 int pf_swap(pf_ctx* ctx);
 
+/* No counterpart in the reference.  pf_diagnosticos without any device
+   allocation, for callers that cannot let a library allocate device memory
+   (a program whose device memory belongs to another runtime, such as an
+   OpenMP target-offload build that passes `use_device_addr` pointers of its
+   mapped fields, or a solver under a fixed device-memory budget).  The
+   caller passes its own device fields (Fortran order, row pitch `pitch` >=
+   nx elements, PF_FP64 doubles or PF_FP32 floats) and receives the five
+   values of pf_diagnosticos in out[5] (host).  Scratch is a static device
+   array of PF_NOALLOC_MAX_PLANES rows (about 256 KiB per device, held until
+   the process exits): nz above that limit is rejected with PF_E_ARG.  The
+   first call on each device looks up the array's device address, so make it
+   before any stream capture.  All calls share the array: calls whose work
+   overlaps on the GPU race.  `stream` is a cudaStream_t or NULL.          */
+#define PF_NOALLOC_MAX_PLANES 4096
+int pf_diagnosticos_noalloc(const void* phase_field, const void* conc_soluto, int nx, int ny, int nz,
+                            int pitch, int precision, double dx, double dy, double dz, double E0,
+                            double W0, void* stream, double out[5]);
+
 /* ---- fused step ------------------------------------------------------- */
 /* Runs n_steps whole iterations of principal.f90:93-226 (temperatura, TP
    ramp, n_varreduras sweeps, solute, auxiliar, swap) with the fused

@@ -30,6 +30,11 @@ int set_global_err(int code, const std::string& msg)
 }
 }  // namespace
 
+namespace pf3d {
+// lets other translation units report through pf_last_error(NULL)
+int set_last_error_global(int code, const std::string& msg) { return set_global_err(code, msg); }
+}  // namespace pf3d
+
 struct pf_ctx {
     pf_grid g;
     pf_params p;

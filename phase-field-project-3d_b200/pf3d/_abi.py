@@ -17,6 +17,7 @@ FIELD_NAMES = ("phase_field_old", "phase_field_new", "conc_soluto_old", "conc_so
 PF_FP64, PF_FP32 = 64, 32
 PF_BC_REFERENCE = 0
 PF_OPT_FUSED, PF_OPT_TILE_Y, PF_OPT_ZCHUNK, PF_OPT_KTIMING = 1, 2, 3, 4
+PF_NOALLOC_MAX_PLANES = 4096
 
 
 class pf_grid(C.Structure):
@@ -80,6 +81,8 @@ SIGNATURES = [
     ("pf_swap", C.c_int, [_P]),
     ("pf_step", C.c_int, [_P, C.c_int]),
     ("pf_step_diag", C.c_int, [_P, C.c_int, _D]),
+    ("pf_diagnosticos_noalloc", C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                          C.c_double, C.c_double, C.c_double, C.c_double, _P, _D]),
 ]
 
 
