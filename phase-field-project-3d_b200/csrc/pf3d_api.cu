@@ -103,6 +103,9 @@ static void fill_desc(const pf_grid& g, const pf_params& p, const pf_derived& dv
     d.InvDX = 1.0 / (g.dx * g.dx); d.InvDY = 1.0 / (g.dy * g.dy); d.InvDZ = 1.0 / (g.dz * g.dz);
     d.hx = 0.5 / g.dx; d.hy = 0.5 / g.dy; d.hz = 0.5 / g.dz;
     d.rdx2 = 1.0 / (g.dx * g.dx); d.rdy2 = 1.0 / (g.dy * g.dy); d.rdz2 = 1.0 / (g.dz * g.dz);
+    d.AAA16 = dv.AAA * 16.0;
+    d.omKe = 1.0 - (double)p.Ke;
+    d.dtIX = dv.DELTA_T * d.InvDX; d.dtIY = dv.DELTA_T * d.InvDY; d.dtIZ = dv.DELTA_T * d.InvDZ;
     d.hq = p.h_quintico;
     d.rt = p.ruido_tipo;
     d.do_heat_lap = (p.D != 0.0) ? 1 : 0;
@@ -121,6 +124,7 @@ static StepArgs make_step_args(const pf_ctx* c, int it, double TP_heat, double T
     s.RTV = c->p.R * TP / c->p.Vm;
     s.omCs = 1.0 - Cs;
     s.omCl = 1.0 - Cl;
+    s.Lc = std::log(s.omCs / s.omCl);
     return s;
 }
 

@@ -35,10 +35,11 @@ struct DomainDesc {
     double cxy, cyz, czx;         // 0.25/(dx*dy), 0.25/(dy*dz), 0.25/(dz*dx)
     double dx2, dy2, dz2;         // dx**2 ...
     double InvDX, InvDY, InvDZ;   // 1/(DX*DX) ... (concentracao_soluto.f90:9-11)
-    double fl_dE;                 // FP32 only: 0.5/dx, 0.5/dy, 0.5/dz packed below
-    double hx, hy, hz;            // 0.5/dx, 0.5/dy, 0.5/dz (FP32 gradients)
-    double rdx2, rdy2, rdz2;      // 1/dx^2 ... (FP32)
-    double dE_scale;              // 0.5*E0*E0*dx*dy*dz factor pieces (diagnostics)
+    double hx, hy, hz;            // 0.5/dx, 0.5/dy, 0.5/dz (fast-form gradients)
+    double rdx2, rdy2, rdz2;      // 1/dx^2 ... (fast form)
+    double AAA16;                 // AAA*16 (fast form)
+    double omKe;                  // 1 - Ke (fast form)
+    double dtIX, dtIY, dtIZ;      // DELTA_T*InvDX ... (fast form)
     int hq;                       // h_quintico
     int rt;                       // ruido_tipo
     int do_heat_lap;              // D != 0
@@ -53,6 +54,7 @@ struct StepArgs {
     double M0dt;         // M0*DELTA_T (phase_body.inc:194)
     double RTV;          // R*TP/Vm (phase_body.inc:174)
     double omCs, omCl;   // 1-Cs_eq, 1-Cl_eq
+    double Lc;           // log((1-Cs_eq)/(1-Cl_eq)) (fast form of phase_body.inc:174)
 };
 
 // ---------------------------------------------------------------------------
@@ -127,6 +129,7 @@ struct KC {
     T cxy, cyz, czx, dx2, dy2, dz2, InvDX, InvDY, InvDZ;
     T hx, hy, hz, rdx2, rdy2, rdz2;
     T TP, TP_heat, M0dt, RTV, omCs, omCl;
+    T AAA16, omKe, dtIX, dtIY, dtIZ, Lc;
     int hq, rt, it, lap;
     __device__ __forceinline__ void load(const DomainDesc& d, const StepArgs& s)
     {
@@ -141,15 +144,28 @@ struct KC {
         rdx2 = (T)d.rdx2; rdy2 = (T)d.rdy2; rdz2 = (T)d.rdz2;
         TP = (T)s.TP; TP_heat = (T)s.TP_heat; M0dt = (T)s.M0dt; RTV = (T)s.RTV;
         omCs = (T)s.omCs; omCl = (T)s.omCl;
+        AAA16 = (T)d.AAA16; omKe = (T)d.omKe; dtIX = (T)d.dtIX; dtIY = (T)d.dtIY; dtIZ = (T)d.dtIZ;
+        Lc = (T)s.Lc;
         hq = d.hq; rt = d.rt; it = s.it; lap = d.do_heat_lap;
     }
 };
 
+// ---------------------------------------------------------------------------
+// Per-cell arithmetic.  FAST = false is the reference form (statement order of
+// the Fortran, IEEE divisions; FP64 kernels built without contraction).
+// FAST = true is the fast form used by the fused passes: the same equations,
+// divisions by grid constants replaced by products with host-rounded
+// reciprocals, one reciprocal per shared denominator, the cross terms grouped
+// by node, and the log argument of phase_body.inc:174 reduced to
+// (den - c)/(den - Ke c) plus a per-step constant.  In FP64 it stays within
+// 1e-12 of the reference form after thousands of steps (tests).
+// ---------------------------------------------------------------------------
+
 // node-centred central gradient component: (a-b)*0.5d0/dx (phase_body.inc:55-122)
-template <typename T>
+template <typename T, bool FAST>
 __device__ __forceinline__ T grad(T a, T b, T d, T half_inv)
 {
-    if constexpr (sizeof(T) == 8) return (a - b) * (T)0.5 / d;
+    if constexpr (!FAST) return (a - b) * (T)0.5 / d;
     else return (a - b) * half_inv;
 }
 
@@ -158,7 +174,7 @@ __device__ __forceinline__ T grad(T a, T b, T d, T half_inv)
 template <typename T>
 struct Node { T eps, exy, eyz, ezx; };
 
-template <typename T>
+template <typename T, bool FAST>
 __device__ __forceinline__ Node<T> aniso_node(T gx, T gy, T gz, const KC<T>& c)
 {
     Node<T> n;
@@ -166,7 +182,7 @@ __device__ __forceinline__ Node<T> aniso_node(T gx, T gy, T gz, const KC<T>& c)
     T Q = gx2 + gy2 + gz2 + (T)1e-23;
     T S4 = gx2 * gx2 + gy2 * gy2 + gz2 * gz2;
     T Q2 = Q * Q;
-    if constexpr (sizeof(T) == 8) {
+    if constexpr (!FAST) {
         n.eps = c.E0 * ((T)1 + c.DE * ((T)4 * S4 / Q2 - (T)3));
         T Ke_ = c.K * n.eps;
         n.exy = Ke_ * gx * gy * (gx2 - gy2) / Q2;
@@ -175,10 +191,10 @@ __device__ __forceinline__ Node<T> aniso_node(T gx, T gy, T gz, const KC<T>& c)
     } else {
         T rq = Ar<T>::rcp(Q2);
         n.eps = c.E0 * ((T)1 + c.DE * ((T)4 * S4 * rq - (T)3));
-        T Ke_ = c.K * n.eps * rq;
-        n.exy = Ke_ * gx * gy * (gx2 - gy2);
-        n.eyz = Ke_ * gy * gz * (gy2 - gz2);
-        n.ezx = Ke_ * gz * gx * (gz2 - gx2);
+        T f = c.K * n.eps * rq;
+        n.exy = f * gx * gy * (gx2 - gy2);
+        n.eyz = f * gy * gz * (gy2 - gz2);
+        n.ezx = f * gz * gx * (gz2 - gx2);
     }
     return n;
 }
@@ -192,74 +208,80 @@ struct Nbr {
 
 // phase_body.inc:133-198 given the stencil values and the six node
 // quantities.  Returns PPNEW (unclamped).
-template <typename T>
+template <typename T, bool FAST>
 __device__ __forceinline__ T phase_ppnew(const Nbr<T>& p, const Node<T>& E, const Node<T>& W, const Node<T>& N,
                                           const Node<T>& S, const Node<T>& Tt, const Node<T>& B, T CPP,
                                           float ran, const KC<T>& c)
 {
     const T PP = p.PP;
-    T AA, Cxy, Cyz, Czx;
-    if constexpr (sizeof(T) == 8) {
-        AA = (E.eps * E.eps * (p.PE - PP) + W.eps * W.eps * (p.PW - PP)) / c.dx2 +
-             (N.eps * N.eps * (p.PN - PP) + S.eps * S.eps * (p.PS - PP)) / c.dy2 +
-             (Tt.eps * Tt.eps * (p.PT - PP) + B.eps * B.eps * (p.PB - PP)) / c.dz2;
-        Cxy = c.cxy * (p.PNE * (-N.exy - (-E.exy)) + p.PSE * (-E.exy - (-S.exy)) + p.PNW * (-W.exy - (-N.exy)) +
-                       p.PSW * (-S.exy - (-W.exy))) +
-              p.PN * c.cxy * (-W.exy - (-E.exy)) + p.PS * c.cxy * (-E.exy - (-W.exy)) +
-              p.PE * c.cxy * (-N.exy - (-S.exy)) + p.PW * c.cxy * (-S.exy - (-N.exy));
-        Cyz = c.cyz * (p.PNT * (-Tt.eyz - (-N.eyz)) + p.PNB * (-N.eyz - (-B.eyz)) + p.PST * (-S.eyz - (-Tt.eyz)) +
-                       p.PSB * (-B.eyz - (-S.eyz))) +
-              p.PT * c.cyz * (-S.eyz - (-N.eyz)) + p.PB * c.cyz * (-N.eyz - (-S.eyz)) +
-              p.PN * c.cyz * (-Tt.eyz - (-B.eyz)) + p.PS * c.cyz * (-B.eyz - (-Tt.eyz));
-        Czx = c.czx * (p.PET * (-E.ezx - (-Tt.ezx)) + p.PWT * (-Tt.ezx - (-W.ezx)) + p.PEB * (-B.ezx - (-E.ezx)) +
-                       p.PWB * (-W.ezx - (-B.ezx))) +
-              p.PE * c.czx * (-B.ezx - (-Tt.ezx)) + p.PW * c.czx * (-Tt.ezx - (-B.ezx)) +
-              p.PT * c.czx * (-E.ezx - (-W.ezx)) + p.PB * c.czx * (-W.ezx - (-E.ezx));
-    } else {
-        AA = (E.eps * E.eps * (p.PE - PP) + W.eps * W.eps * (p.PW - PP)) * c.rdx2 +
-             (N.eps * N.eps * (p.PN - PP) + S.eps * S.eps * (p.PS - PP)) * c.rdy2 +
-             (Tt.eps * Tt.eps * (p.PT - PP) + B.eps * B.eps * (p.PB - PP)) * c.rdz2;
-        Cxy = c.cxy * (p.PNE * (E.exy - N.exy) + p.PSE * (S.exy - E.exy) + p.PNW * (N.exy - W.exy) +
-                       p.PSW * (W.exy - S.exy) + p.PN * (E.exy - W.exy) + p.PS * (W.exy - E.exy) +
-                       p.PE * (S.exy - N.exy) + p.PW * (N.exy - S.exy));
-        Cyz = c.cyz * (p.PNT * (N.eyz - Tt.eyz) + p.PNB * (B.eyz - N.eyz) + p.PST * (Tt.eyz - S.eyz) +
-                       p.PSB * (S.eyz - B.eyz) + p.PT * (N.eyz - S.eyz) + p.PB * (S.eyz - N.eyz) +
-                       p.PN * (B.eyz - Tt.eyz) + p.PS * (Tt.eyz - B.eyz));
-        Czx = c.czx * (p.PET * (Tt.ezx - E.ezx) + p.PWT * (W.ezx - Tt.ezx) + p.PEB * (E.ezx - B.ezx) +
-                       p.PWB * (B.ezx - W.ezx) + p.PE * (Tt.ezx - B.ezx) + p.PW * (B.ezx - Tt.ezx) +
-                       p.PT * (W.ezx - E.ezx) + p.PB * (E.ezx - W.ezx));
-    }
-    AA = AA + Cxy + Cyz + Czx;
-
     const T one = (T)1, two = (T)2;
-    T g_linha = two * PP * (one - PP) * (one - PP) - two * PP * PP * (one - PP);
-    T h_linha, h;
-    if (c.hq == 1) {
-        h_linha = (T)30 * PP * PP * (one - PP) * (one - PP);
-        h = PP * PP * PP * ((T)10 - (T)15 * PP + (T)6 * PP * PP);
+    if constexpr (!FAST) {
+        T AA = (E.eps * E.eps * (p.PE - PP) + W.eps * W.eps * (p.PW - PP)) / c.dx2 +
+               (N.eps * N.eps * (p.PN - PP) + S.eps * S.eps * (p.PS - PP)) / c.dy2 +
+               (Tt.eps * Tt.eps * (p.PT - PP) + B.eps * B.eps * (p.PB - PP)) / c.dz2;
+        T Cxy = c.cxy * (p.PNE * (-N.exy - (-E.exy)) + p.PSE * (-E.exy - (-S.exy)) + p.PNW * (-W.exy - (-N.exy)) +
+                         p.PSW * (-S.exy - (-W.exy))) +
+                p.PN * c.cxy * (-W.exy - (-E.exy)) + p.PS * c.cxy * (-E.exy - (-W.exy)) +
+                p.PE * c.cxy * (-N.exy - (-S.exy)) + p.PW * c.cxy * (-S.exy - (-N.exy));
+        T Cyz = c.cyz * (p.PNT * (-Tt.eyz - (-N.eyz)) + p.PNB * (-N.eyz - (-B.eyz)) + p.PST * (-S.eyz - (-Tt.eyz)) +
+                         p.PSB * (-B.eyz - (-S.eyz))) +
+                p.PT * c.cyz * (-S.eyz - (-N.eyz)) + p.PB * c.cyz * (-N.eyz - (-S.eyz)) +
+                p.PN * c.cyz * (-Tt.eyz - (-B.eyz)) + p.PS * c.cyz * (-B.eyz - (-Tt.eyz));
+        T Czx = c.czx * (p.PET * (-E.ezx - (-Tt.ezx)) + p.PWT * (-Tt.ezx - (-W.ezx)) + p.PEB * (-B.ezx - (-E.ezx)) +
+                         p.PWB * (-W.ezx - (-B.ezx))) +
+                p.PE * c.czx * (-B.ezx - (-Tt.ezx)) + p.PW * c.czx * (-Tt.ezx - (-B.ezx)) +
+                p.PT * c.czx * (-E.ezx - (-W.ezx)) + p.PB * c.czx * (-W.ezx - (-E.ezx));
+        AA = AA + Cxy + Cyz + Czx;
+        T g_linha = two * PP * (one - PP) * (one - PP) - two * PP * PP * (one - PP);
+        T h_linha, h;
+        if (c.hq == 1) {
+            h_linha = (T)30 * PP * PP * (one - PP) * (one - PP);
+            h = PP * PP * PP * ((T)10 - (T)15 * PP + (T)6 * PP * PP);
+        } else {
+            h_linha = two * PP * ((T)3 - two * PP) - two * PP * PP;
+            h = PP * PP * ((T)3 - two * PP);
+        }
+        T den = c.Ke * h + (one - h);
+        T CLP = CPP / den;
+        T CSP = c.Ke * CPP / den;
+        T GG = (-(c.W0 * g_linha)) + c.RTV * h_linha * log(fabs(c.omCs * (one - CLP) / (c.omCl * (one - CSP))));
+        T pp2 = PP * PP, q = one - PP;
+        T ruidos;
+        if (c.rt == 0)
+            ruidos = (T)ran * c.AAA * (T)16 * pp2 * (q * q);
+        else
+            ruidos = (two * (T)ran - one) * c.AAA * (T)16 * pp2 * (q * q);
+        return PP + c.M0dt * (AA + GG) + ruidos;
     } else {
-        h_linha = two * PP * ((T)3 - two * PP) - two * PP * PP;
-        h = PP * PP * ((T)3 - two * PP);
+        T AA = (E.eps * E.eps * (p.PE - PP) + W.eps * W.eps * (p.PW - PP)) * c.rdx2 +
+               (N.eps * N.eps * (p.PN - PP) + S.eps * S.eps * (p.PS - PP)) * c.rdy2 +
+               (Tt.eps * Tt.eps * (p.PT - PP) + B.eps * B.eps * (p.PB - PP)) * c.rdz2;
+        // cross terms of phase_body.inc:137-147 grouped by node
+        T Cxy = E.exy * (p.PNE - p.PSE + p.PN - p.PS) + N.exy * (p.PNW - p.PNE + p.PW - p.PE) +
+                W.exy * (p.PSW - p.PNW + p.PS - p.PN) + S.exy * (p.PSE - p.PSW + p.PE - p.PW);
+        T Cyz = N.eyz * (p.PNT - p.PNB + p.PT - p.PB) + Tt.eyz * (p.PST - p.PNT + p.PS - p.PN) +
+                S.eyz * (p.PSB - p.PST + p.PB - p.PT) + B.eyz * (p.PNB - p.PSB + p.PN - p.PS);
+        T Czx = Tt.ezx * (p.PET - p.PWT + p.PE - p.PW) + W.ezx * (p.PWT - p.PWB + p.PT - p.PB) +
+                B.ezx * (p.PWB - p.PEB + p.PW - p.PE) + E.ezx * (p.PEB - p.PET + p.PB - p.PT);
+        AA = AA + c.cxy * Cxy + c.cyz * Cyz + c.czx * Czx;
+        const T q = one - PP;
+        T g_linha = two * PP * q * (one - two * PP);
+        T h_linha, h;
+        if (c.hq == 1) {
+            h_linha = (T)30 * PP * PP * q * q;
+            h = PP * PP * PP * ((T)10 - (T)15 * PP + (T)6 * PP * PP);
+        } else {
+            h_linha = (T)6 * PP * q;
+            h = PP * PP * ((T)3 - two * PP);
+        }
+        T den = one - c.omKe * h;
+        // (1-CLP)/(1-CSP) = (den - c)/(den - Ke c); the constant factor is in Lc
+        T lg = Ar<T>::lg(fabs(Ar<T>::div(den - CPP, den - c.Ke * CPP))) + c.Lc;
+        T GG = c.RTV * h_linha * lg - c.W0 * g_linha;
+        T pp2q2 = PP * PP * q * q * c.AAA16;
+        T ruidos = (c.rt == 0) ? (T)ran * pp2q2 : (two * (T)ran - one) * pp2q2;
+        return PP + c.M0dt * (AA + GG) + ruidos;
     }
-    T den = c.Ke * h + (one - h);
-    T CLP, CSP;
-    if constexpr (sizeof(T) == 8) {
-        CLP = CPP / den;
-        CSP = c.Ke * CPP / den;
-    } else {
-        T rd = Ar<T>::rcp(den);
-        CLP = CPP * rd;
-        CSP = c.Ke * CPP * rd;
-    }
-    T GG = (-(c.W0 * g_linha)) +
-           c.RTV * h_linha * Ar<T>::lg(fabs(Ar<T>::div(c.omCs * (one - CLP), c.omCl * (one - CSP))));
-    T pp2 = PP * PP, q = one - PP;
-    T ruidos;
-    if (c.rt == 0)
-        ruidos = (T)ran * c.AAA * (T)16 * pp2 * (q * q);
-    else
-        ruidos = (two * (T)ran - one) * c.AAA * (T)16 * pp2 * (q * q);
-    return PP + c.M0dt * (AA + GG) + ruidos;
 }
 
 // dmax1(0, dmin1(1, x)) (phase_body.inc:198)
@@ -279,53 +301,67 @@ __device__ __forceinline__ T h_conc(T P, int hq)
     return P * P * ((T)3 - (T)2 * P);
 }
 
-// Per-point solute quantities of conc_body.inc: CL, the Gamma bracket
-// (1-h)CL(1-CL)+h CS(1-CS), and mu = log(CL/(1-CL)).
+// Per-point solute quantities of conc_body.inc: the Gamma bracket
+// (1-h)CL(1-CL)+h CS(1-CS) and mu = log(CL/(1-CL)).
 template <typename T>
 struct SolNode { T br, mu; };
 
-template <typename T>
+template <typename T, bool FAST>
 __device__ __forceinline__ SolNode<T> sol_node(T P, T C, const KC<T>& c)
 {
     const T one = (T)1;
     T h = h_conc(P, c.hq);
-    T den = (c.Ke * h) + (one - h);
-    T CS, CL;
-    if constexpr (sizeof(T) == 8) {
-        CS = (c.Ke * C) / den;
-        CL = C / den;
-    } else {
-        T rd = Ar<T>::rcp(den);
-        CS = c.Ke * C * rd;
-        CL = C * rd;
-    }
     SolNode<T> n;
-    n.br = (one - h) * CL * (one - CL) + h * CS * (one - CS);
-    n.mu = Ar<T>::lg(Ar<T>::div(CL, one - CL));
+    if constexpr (!FAST) {
+        T den = (c.Ke * h) + (one - h);
+        T CS = (c.Ke * C) / den;
+        T CL = C / den;
+        n.br = (one - h) * CL * (one - CL) + h * CS * (one - CS);
+        n.mu = log(CL / (one - CL));
+    } else {
+        T den = one - c.omKe * h;
+        T CL = C * Ar<T>::rcp(den);
+        T CS = c.Ke * CL;
+        n.br = (one - h) * CL * (one - CL) + h * CS * (one - CS);
+        n.mu = Ar<T>::lg(Ar<T>::div(C, den - C));   // CL/(1-CL) = C/(den-C)
+    }
     return n;
 }
 
 // conc_body.inc:92-149 given the seven per-point quantities.
-template <typename T>
+template <typename T, bool FAST>
 __device__ __forceinline__ T conc_new(T PP, T CPP, const SolNode<T>& P, const SolNode<T>& E, const SolNode<T>& W,
                                       const SolNode<T>& N, const SolNode<T>& S, const SolNode<T>& Tt,
                                       const SolNode<T>& B, const KC<T>& c)
 {
     const T Dc = (PP <= (T)0.95) ? c.D_liq : c.D_sol;
-    const T two = (T)2, one = (T)1;
-    T GP = Dc * P.br, GS = Dc * S.br, GN = Dc * N.br, GW = Dc * W.br, GE = Dc * E.br, GT = Dc * Tt.br, GB = Dc * B.br;
-    T iP = Ar<T>::rcp(GP);
-    T Gs = Ar<T>::div(two, iP + Ar<T>::rcp(GS));
-    T Gn = Ar<T>::div(two, Ar<T>::rcp(GN) + iP);
-    T Gw = Ar<T>::div(two, iP + Ar<T>::rcp(GW));
-    T Ge = Ar<T>::div(two, Ar<T>::rcp(GE) + iP);
-    T Gt = Ar<T>::div(two, Ar<T>::rcp(GT) + iP);
-    T Gb = Ar<T>::div(two, iP + Ar<T>::rcp(GB));
-    (void)one;
-    return (Ge * c.InvDX * (E.mu - P.mu) - Gw * c.InvDX * (P.mu - W.mu) + Gn * c.InvDY * (N.mu - P.mu) -
-            Gs * c.InvDY * (P.mu - S.mu) + Gt * c.InvDZ * (Tt.mu - P.mu) - Gb * c.InvDZ * (P.mu - B.mu)) *
-               c.dt +
-           CPP;
+    const T two = (T)2;
+    if constexpr (!FAST) {
+        T GP = Dc * P.br, GS = Dc * S.br, GN = Dc * N.br, GW = Dc * W.br, GE = Dc * E.br, GT = Dc * Tt.br,
+          GB = Dc * B.br;
+        T iP = (T)1 / GP;
+        T Gs = two / (iP + (T)1 / GS);
+        T Gn = two / ((T)1 / GN + iP);
+        T Gw = two / (iP + (T)1 / GW);
+        T Ge = two / ((T)1 / GE + iP);
+        T Gt = two / ((T)1 / GT + iP);
+        T Gb = two / (iP + (T)1 / GB);
+        return (Ge * c.InvDX * (E.mu - P.mu) - Gw * c.InvDX * (P.mu - W.mu) + Gn * c.InvDY * (N.mu - P.mu) -
+                Gs * c.InvDY * (P.mu - S.mu) + Gt * c.InvDZ * (Tt.mu - P.mu) - Gb * c.InvDZ * (P.mu - B.mu)) *
+                   c.dt +
+               CPP;
+    } else {
+        // 2/(1/(Dc a) + 1/(Dc b)) = 2 Dc a b / (a + b)
+        const T D2 = two * Dc * P.br;
+        auto hm = [&](T b) -> T {
+            T sum = P.br + b;
+            return (sum > (T)0) ? D2 * b * Ar<T>::rcp(sum) : (T)0;
+        };
+        T fx = hm(E.br) * (E.mu - P.mu) - hm(W.br) * (P.mu - W.mu);
+        T fy = hm(N.br) * (N.mu - P.mu) - hm(S.br) * (P.mu - S.mu);
+        T fz = hm(Tt.br) * (Tt.mu - P.mu) - hm(B.br) * (P.mu - B.mu);
+        return CPP + (c.dtIX * fx + c.dtIY * fy + c.dtIZ * fz);
+    }
 }
 
 // temp_body.inc:31-41 at an interior cell.
@@ -340,11 +376,7 @@ __device__ __forceinline__ T heat_new(T PP, T dpp, T TE, T TW, T TN, T TS, T TT,
     T FONTE = c.dH_cp * h_linha * dpp;
     if (c.lap) {
         T TP = c.TP_heat;
-        T lap;
-        if constexpr (sizeof(T) == 8)
-            lap = ((TE - (T)2 * TP + TW) / c.dx2) + ((TN - (T)2 * TP + TS) / c.dy2) + ((TT - (T)2 * TP + TB) / c.dz2);
-        else
-            lap = ((TE - (T)2 * TP + TW) * c.rdx2) + ((TN - (T)2 * TP + TS) * c.rdy2) + ((TT - (T)2 * TP + TB) * c.rdz2);
+        T lap = ((TE - (T)2 * TP + TW) / c.dx2) + ((TN - (T)2 * TP + TS) / c.dy2) + ((TT - (T)2 * TP + TB) / c.dz2);
         return c.Ddt * lap + FONTE + TP;
     }
     // D = 0: D*DELTA_T*(finite) is a signed zero and drops out exactly.

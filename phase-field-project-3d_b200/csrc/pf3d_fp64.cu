@@ -1,16 +1,14 @@
-// pf3d_fp64.cu -- FP64 (plain form) instantiation of every kernel.
+// pf3d_fp64.cu -- FP64 per-subroutine kernels (reference form), diagnostics and
+// staging conversions.
 // Built with --fmad=false: the reference's gfortran arithmetic on x86-64 has
 // no fused multiply-add, so neither may this form.
 #include "pf3d_simple.cuh"
-#include "pf3d_fused.cuh"
 
 namespace pf3d {
 template cudaError_t launch_heat<double>(const DomainDesc&, const StepArgs&, const Fields&, cudaStream_t);
 template cudaError_t launch_phase<double>(const DomainDesc&, const StepArgs&, const void*, const void*, void*, void*, cudaStream_t);
 template cudaError_t launch_solute<double>(const DomainDesc&, const StepArgs&, const void*, const void*, void*, cudaStream_t);
 template cudaError_t launch_copy_inner<double>(const DomainDesc&, const void*, void*, cudaStream_t);
-template cudaError_t launch_fused_first<double>(const DomainDesc&, const StepArgs&, const Fields&, bool, int, int, cudaStream_t);
-template cudaError_t launch_fused_last<double>(const DomainDesc&, const StepArgs&, const Fields&, int, int, cudaStream_t);
 template cudaError_t launch_diag<double>(const DomainDesc&, const void*, const void*, double*, int, double*, cudaStream_t);
 template cudaError_t launch_convert_in<double>(const DomainDesc&, const double*, void*, long long, long long, cudaStream_t);
 template cudaError_t launch_convert_out<double>(const DomainDesc&, const void*, double*, long long, long long, cudaStream_t);

@@ -18,7 +18,8 @@
 //   DPPW : write DPP (only the last sweep of a step needs to)
 //   SOL  : concentracao_soluto from the same input phase field
 // Every output is written with the closed-form boundary decoration, so one
-// pass replaces the reference's copy + stencil + plane-copy kernels.
+// pass replaces the reference's copy + stencil + plane-copy kernels.  The
+// per-cell arithmetic is the fast form of pf3d_device.cuh (FAST = true).
 #pragma once
 #include "pf3d_launch.h"
 
@@ -78,12 +79,30 @@ __global__ void __launch_bounds__(32 * TY, (TY <= 8) ? 2 : 1) k_fused(DomainDesc
         if (z < 0 || z >= nz) return;
         T(*dst)[PW] = sm.phi[slot5(z)];
         const T* src = phi_in + (long long)z * pl;
-        for (int q = tid; q < PH * PW; q += NT) {
-            int ly = q / PW, lx = q - ly * PW;
-            int gx = x0 - 2 + lx, gy = y0 - 2 + ly;
-            if (gx >= 0 && gx < nx && gy >= 0 && gy < ny)
-                cp_async_elem(&dst[ly][lx], src + gx + (long long)gy * px, (int)sizeof(T));
+        for (int ly = ty; ly < PH; ly += TY) {
+            const int gy = y0 - 2 + ly;
+            if (gy < 0 || gy >= ny) continue;
+            const T* row = src + (long long)gy * px;
+            int gx = x0 - 2 + tx;
+            if (gx >= 0 && gx < nx) cp_async_elem(&dst[ly][tx], row + gx, (int)sizeof(T));
+            if (tx < 4) {
+                gx = x0 + 30 + tx;
+                if (gx < nx) cp_async_elem(&dst[ly][32 + tx], row + gx, (int)sizeof(T));
+            }
         }
+    };
+
+    // node-tile position of the ring item r (0 <= r < RING): the two full
+    // rows above and below the tile, then the two side columns
+    constexpr int RING = 2 * NW + 2 * TY;
+    auto ring_pos = [](int r, int& lx, int& ly) {
+        if (r < NW) { lx = r; ly = 0; return; }
+        r -= NW;
+        if (r < NW) { lx = r; ly = NH - 1; return; }
+        r -= NW;
+        if (r < TY) { lx = 0; ly = 1 + r; return; }
+        r -= TY;
+        lx = NW - 1; ly = 1 + r;
     };
 
     // anisotropy quantities of node plane zn over the tile + ring
@@ -93,19 +112,24 @@ __global__ void __launch_bounds__(32 * TY, (TY <= 8) ? 2 : 1) k_fused(DomainDesc
         const T(*p0)[PW] = sm.phi[slot5(zn)];
         const T(*pp)[PW] = sm.phi[slot5(zn + 1)];
         const int sl = slot3(zn);
-        for (int q = tid; q < NH * NW; q += NT) {
-            int ly = q / NW, lx = q - ly * NW;
+        auto one_node = [&](int lx, int ly) {
             int gx = x0 - 1 + lx, gy = y0 - 1 + ly;
-            if (gx < 1 || gx > nx - 2 || gy < 1 || gy > ny - 2) continue;
+            if (gx < 1 || gx > nx - 2 || gy < 1 || gy > ny - 2) return;
             int fx = lx + 1, fy = ly + 1;   // phase-tile coordinates of the node
-            T gxv = grad<T>(p0[fy][fx + 1], p0[fy][fx - 1], c.dx, c.hx);
-            T gyv = grad<T>(p0[fy + 1][fx], p0[fy - 1][fx], c.dy, c.hy);
-            T gzv = grad<T>(pp[fy][fx], pm[fy][fx], c.dz, c.hz);
-            Node<T> n = aniso_node<T>(gxv, gyv, gzv, c);
+            T gxv = grad<T, true>(p0[fy][fx + 1], p0[fy][fx - 1], c.dx, c.hx);
+            T gyv = grad<T, true>(p0[fy + 1][fx], p0[fy - 1][fx], c.dy, c.hy);
+            T gzv = grad<T, true>(pp[fy][fx], pm[fy][fx], c.dz, c.hz);
+            Node<T> n = aniso_node<T, true>(gxv, gyv, gzv, c);
             sm.eps[sl][ly][lx] = n.eps;
             sm.exy[sl][ly][lx] = n.exy;
             sm.eyz[sl][ly][lx] = n.eyz;
             sm.ezx[sl][ly][lx] = n.ezx;
+        };
+        one_node(tx + 1, ty + 1);
+        if (tid < RING) {
+            int lx, ly;
+            ring_pos(tid, lx, ly);
+            one_node(lx, ly);
         }
     };
 
@@ -116,13 +140,18 @@ __global__ void __launch_bounds__(32 * TY, (TY <= 8) ? 2 : 1) k_fused(DomainDesc
         const T(*p0)[PW] = sm.phi[slot5(zs)];
         const int sl = slot3(zs);
         const T* cz = c_in + (long long)zs * pl;
-        for (int q = tid; q < NH * NW; q += NT) {
-            int ly = q / NW, lx = q - ly * NW;
+        auto one_point = [&](int lx, int ly) {
             int gx = x0 - 1 + lx, gy = y0 - 1 + ly;
-            if (gx < 0 || gx > nx - 1 || gy < 0 || gy > ny - 1) continue;
-            SolNode<T> n = sol_node<T>(p0[ly + 1][lx + 1], cz[gx + (long long)gy * px], c);
+            if (gx < 0 || gx > nx - 1 || gy < 0 || gy > ny - 1) return;
+            SolNode<T> n = sol_node<T, true>(p0[ly + 1][lx + 1], cz[gx + (long long)gy * px], c);
             sm.br[sl][ly][lx] = n.br;
             sm.mu[sl][ly][lx] = n.mu;
+        };
+        one_point(tx + 1, ty + 1);
+        if (tid < RING) {
+            int lx, ly;
+            ring_pos(tid, lx, ly);
+            one_point(lx, ly);
         }
     };
 
@@ -200,7 +229,7 @@ __global__ void __launch_bounds__(32 * TY, (TY <= 8) ? 2 : 1) k_fused(DomainDesc
                     B.eps = sm.eps[sm1][nly][nlx]; B.eyz = sm.eyz[sm1][nly][nlx]; B.ezx = sm.ezx[sm1][nly][nlx];
                     E.eyz = W.eyz = N.ezx = S.ezx = Tt.exy = B.exy = (T)0;   // unused by the body
                     float ran = phase_ran(c.rt, x + 1, y + 1, z + 1, c.it);
-                    T ppn = phase_ppnew<T>(nb, E, W, N, S, Tt, B, c_in[id], ran, c);
+                    T ppn = phase_ppnew<T, true>(nb, E, W, N, S, Tt, B, c_in[id], ran, c);
                     if (DPPW) dpp[id] = ppn - PPc;
                     U = clamp01(ppn);
                 } else {
@@ -230,7 +259,7 @@ __global__ void __launch_bounds__(32 * TY, (TY <= 8) ? 2 : 1) k_fused(DomainDesc
                         SolNode<T> nS{sm.br[s0][nly - 1][nlx], sm.mu[s0][nly - 1][nlx]};
                         SolNode<T> nT{sm.br[sp][nly][nlx], sm.mu[sp][nly][nlx]};
                         SolNode<T> nB{sm.br[sm1][nly][nlx], sm.mu[sm1][nly][nlx]};
-                        Uc = conc_new<T>(PPc, c_in[id], nP, nE, nW, nN, nS, nT, nB, c);
+                        Uc = conc_new<T, true>(PPc, c_in[id], nP, nE, nW, nN, nS, nT, nB, c);
                         c_out[id] = Uc;
                     } else {
                         Uc = c_in[id];

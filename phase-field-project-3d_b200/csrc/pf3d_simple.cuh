@@ -47,6 +47,7 @@ __global__ void __launch_bounds__(256) k_phase(DomainDesc d, StepArgs s, const T
     long long id = cell_off(d, x, y, z);
     T U;
     if (x >= 2 && x <= d.nx - 3 && y >= 2 && y <= d.ny - 3 && z >= 2 && z <= d.nz - 3) {
+        constexpr bool FAST = sizeof(T) == 4;   // FP64: the reference form
         KC<T> c;
         c.load(d, s);
         const T* p = po + id;
@@ -59,20 +60,20 @@ __global__ void __launch_bounds__(256) k_phase(DomainDesc d, StepArgs s, const T
         nb.PNE = P(1, 1, 0); nb.PSE = P(1, -1, 0); nb.PNW = P(-1, 1, 0); nb.PSW = P(-1, -1, 0);
         nb.PNT = P(0, 1, 1); nb.PNB = P(0, 1, -1); nb.PST = P(0, -1, 1); nb.PSB = P(0, -1, -1);
         nb.PET = P(1, 0, 1); nb.PEB = P(1, 0, -1); nb.PWT = P(-1, 0, 1); nb.PWB = P(-1, 0, -1);
-        Node<T> E = aniso_node<T>(grad<T>(P(2, 0, 0), nb.PP, c.dx, c.hx), grad<T>(P(1, 1, 0), P(1, -1, 0), c.dy, c.hy),
-                                  grad<T>(P(1, 0, 1), P(1, 0, -1), c.dz, c.hz), c);
-        Node<T> W = aniso_node<T>(grad<T>(nb.PP, P(-2, 0, 0), c.dx, c.hx), grad<T>(P(-1, 1, 0), P(-1, -1, 0), c.dy, c.hy),
-                                  grad<T>(P(-1, 0, 1), P(-1, 0, -1), c.dz, c.hz), c);
-        Node<T> N = aniso_node<T>(grad<T>(P(1, 1, 0), P(-1, 1, 0), c.dx, c.hx), grad<T>(P(0, 2, 0), nb.PP, c.dy, c.hy),
-                                  grad<T>(P(0, 1, 1), P(0, 1, -1), c.dz, c.hz), c);
-        Node<T> S = aniso_node<T>(grad<T>(P(1, -1, 0), P(-1, -1, 0), c.dx, c.hx), grad<T>(nb.PP, P(0, -2, 0), c.dy, c.hy),
-                                  grad<T>(P(0, -1, 1), P(0, -1, -1), c.dz, c.hz), c);
-        Node<T> Tt = aniso_node<T>(grad<T>(P(1, 0, 1), P(-1, 0, 1), c.dx, c.hx), grad<T>(P(0, 1, 1), P(0, -1, 1), c.dy, c.hy),
-                                   grad<T>(P(0, 0, 2), nb.PP, c.dz, c.hz), c);
-        Node<T> B = aniso_node<T>(grad<T>(P(1, 0, -1), P(-1, 0, -1), c.dx, c.hx), grad<T>(P(0, 1, -1), P(0, -1, -1), c.dy, c.hy),
-                                  grad<T>(nb.PP, P(0, 0, -2), c.dz, c.hz), c);
+        Node<T> E = aniso_node<T, FAST>(grad<T, FAST>(P(2, 0, 0), nb.PP, c.dx, c.hx), grad<T, FAST>(P(1, 1, 0), P(1, -1, 0), c.dy, c.hy),
+                                  grad<T, FAST>(P(1, 0, 1), P(1, 0, -1), c.dz, c.hz), c);
+        Node<T> W = aniso_node<T, FAST>(grad<T, FAST>(nb.PP, P(-2, 0, 0), c.dx, c.hx), grad<T, FAST>(P(-1, 1, 0), P(-1, -1, 0), c.dy, c.hy),
+                                  grad<T, FAST>(P(-1, 0, 1), P(-1, 0, -1), c.dz, c.hz), c);
+        Node<T> N = aniso_node<T, FAST>(grad<T, FAST>(P(1, 1, 0), P(-1, 1, 0), c.dx, c.hx), grad<T, FAST>(P(0, 2, 0), nb.PP, c.dy, c.hy),
+                                  grad<T, FAST>(P(0, 1, 1), P(0, 1, -1), c.dz, c.hz), c);
+        Node<T> S = aniso_node<T, FAST>(grad<T, FAST>(P(1, -1, 0), P(-1, -1, 0), c.dx, c.hx), grad<T, FAST>(nb.PP, P(0, -2, 0), c.dy, c.hy),
+                                  grad<T, FAST>(P(0, -1, 1), P(0, -1, -1), c.dz, c.hz), c);
+        Node<T> Tt = aniso_node<T, FAST>(grad<T, FAST>(P(1, 0, 1), P(-1, 0, 1), c.dx, c.hx), grad<T, FAST>(P(0, 1, 1), P(0, -1, 1), c.dy, c.hy),
+                                   grad<T, FAST>(P(0, 0, 2), nb.PP, c.dz, c.hz), c);
+        Node<T> B = aniso_node<T, FAST>(grad<T, FAST>(P(1, 0, -1), P(-1, 0, -1), c.dx, c.hx), grad<T, FAST>(P(0, 1, -1), P(0, -1, -1), c.dy, c.hy),
+                                  grad<T, FAST>(nb.PP, P(0, 0, -2), c.dz, c.hz), c);
         float ran = phase_ran(c.rt, x + 1, y + 1, z + 1, c.it);
-        T ppn = phase_ppnew<T>(nb, E, W, N, S, Tt, B, co[id], ran, c);
+        T ppn = phase_ppnew<T, FAST>(nb, E, W, N, S, Tt, B, co[id], ran, c);
         dpp[id] = ppn - nb.PP;
         U = clamp01(ppn);
     } else {
@@ -103,18 +104,19 @@ __global__ void __launch_bounds__(256) k_solute(DomainDesc d, StepArgs s, const 
     if (!feeds) return;
     T U;
     if (inner) {
+        constexpr bool FAST = sizeof(T) == 4;
         KC<T> c;
         c.load(d, s);
         const long long sy = d.px, sz = d.plane;
         T PP = po[id];
-        SolNode<T> nP = sol_node<T>(PP, co[id], c);
-        SolNode<T> nE = sol_node<T>(po[id + 1], co[id + 1], c);
-        SolNode<T> nW = sol_node<T>(po[id - 1], co[id - 1], c);
-        SolNode<T> nN = sol_node<T>(po[id + sy], co[id + sy], c);
-        SolNode<T> nS = sol_node<T>(po[id - sy], co[id - sy], c);
-        SolNode<T> nT = sol_node<T>(po[id + sz], co[id + sz], c);
-        SolNode<T> nB = sol_node<T>(po[id - sz], co[id - sz], c);
-        U = conc_new<T>(PP, co[id], nP, nE, nW, nN, nS, nT, nB, c);
+        SolNode<T> nP = sol_node<T, FAST>(PP, co[id], c);
+        SolNode<T> nE = sol_node<T, FAST>(po[id + 1], co[id + 1], c);
+        SolNode<T> nW = sol_node<T, FAST>(po[id - 1], co[id - 1], c);
+        SolNode<T> nN = sol_node<T, FAST>(po[id + sy], co[id + sy], c);
+        SolNode<T> nS = sol_node<T, FAST>(po[id - sy], co[id - sy], c);
+        SolNode<T> nT = sol_node<T, FAST>(po[id + sz], co[id + sz], c);
+        SolNode<T> nB = sol_node<T, FAST>(po[id - sz], co[id - sz], c);
+        U = conc_new<T, FAST>(PP, co[id], nP, nE, nW, nN, nS, nT, nB, c);
         cn[id] = U;
     } else {
         U = co[id];

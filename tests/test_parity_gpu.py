@@ -2,8 +2,9 @@
 
 Plain form (FP64): every field within RTOL_FP64 = 1e-12 (normwise max
 relative) of the oracle after N steps; everything that does not pass through
-`log` is bit-identical (the heat equation, the noise stream).  The fused
-kernels equal the per-subroutine kernels bit for bit.
+`log` is bit-identical in the per-subroutine kernels (the heat equation, the
+noise stream).  The fused passes use the fast FP64 form and are held to the
+same 1e-12 bar.
 """
 import numpy as np
 import pytest
@@ -118,7 +119,10 @@ def test_fused_step_matches_oracle(gpu, shape, over):
 
 
 @pytest.mark.parametrize("tile_y,zchunk", [(4, 0), (8, 64), (16, 7), (8, 1)])
-def test_fused_equals_per_subroutine_bitwise(gpu, tile_y, zchunk):
+def test_fused_matches_per_subroutine(gpu, tile_y, zchunk):
+    """The fused passes (fast FP64 form) against the per-subroutine kernels
+    (reference form): tiling, z-chunking, node reuse and the closed-form
+    decoration must not change anything beyond rounding."""
     g, p, st = small_case(70, 45, 50)
     with pf3d.Domain(g, p) as a, pf3d.Domain(g, p) as b:
         a.load_state(st); b.load_state(st)
@@ -127,9 +131,7 @@ def test_fused_equals_per_subroutine_bitwise(gpu, tile_y, zchunk):
         b.set_option(pf3d.PF_OPT_FUSED, 0)
         a.step(3)
         b.step(3)
-        fa, fb = a.fields(), b.fields()
-        for k in fa:
-            assert np.array_equal(fa[k], fb[k]), k
+        compare(a.fields(), b.fields())
 
 
 def exact_diagnostics(phi, c, dx, dy, dz, E0, w0):
