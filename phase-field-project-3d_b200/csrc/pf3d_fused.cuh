@@ -20,6 +20,11 @@
 // Every output is written with the closed-form boundary decoration, so one
 // pass replaces the reference's copy + stencil + plane-copy kernels.  The
 // per-cell arithmetic is the fast form of pf3d_device.cuh (FAST = true).
+//
+// Latency hiding: the window slots advance incrementally (no modulo), the
+// centre values the cell update reads from global memory (c, DPP) are loaded
+// at the top of the plane iteration, and the concentration values of the
+// next solute plane are loaded one plane ahead into registers.
 #pragma once
 #include "pf3d_launch.h"
 
@@ -46,15 +51,26 @@ struct FusedSmem {
     T br[3][NH][NW], mu[3][NH][NW];
 };
 
+// resident CTAs per SM the register budget is sized for: 16 warps in FP64,
+// 24 in FP32
+template <typename T, int TY>
+struct FusedOcc {
+    static constexpr int warps = (sizeof(T) == 8) ? 16 : 24;
+    static constexpr int v = (warps / TY) > 0 ? (warps / TY) : 1;
+};
+
+__device__ __forceinline__ int add5(int a, int k) { int t = a + k; return t >= 5 ? t - 5 : t; }
+__device__ __forceinline__ int add3(int a, int k) { int t = a + k; return t >= 3 ? t - 3 : t; }
+
 template <typename T, int TY, bool HEAT, bool DPPW, bool SOL>
-__global__ void __launch_bounds__(32 * TY, (TY <= 8) ? 2 : 1) k_fused(DomainDesc d, StepArgs s, const T* __restrict__ phi_in,
-                                                   const T* __restrict__ c_in, T* __restrict__ phi_out,
-                                                   T* __restrict__ dpp, T* __restrict__ c_out,
-                                                   const T* __restrict__ T_old, T* __restrict__ T_new, int zchunk)
+__global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY>::v))
+    k_fused(DomainDesc d, StepArgs s, const T* __restrict__ phi_in, const T* __restrict__ c_in,
+            T* __restrict__ phi_out, T* __restrict__ dpp, T* __restrict__ c_out, const T* __restrict__ T_old,
+            T* __restrict__ T_new, int zchunk)
 {
     using SM = FusedSmem<T, TY>;
     constexpr int TX = SM::TX, PW = SM::PW, PH = SM::PH, NW = SM::NW, NH = SM::NH;
-    constexpr int NT = TX * TY;
+    constexpr int RING = 2 * NW + 2 * TY;   // ring nodes around the tile
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SM& sm = *reinterpret_cast<SM*>(smem_raw);
 
@@ -63,21 +79,39 @@ __global__ void __launch_bounds__(32 * TY, (TY <= 8) ? 2 : 1) k_fused(DomainDesc
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int zb = blockIdx.z * zchunk;
     const int ze = min(zb + zchunk, nz);
-    const int tid = threadIdx.x + TX * threadIdx.y;
     const int tx = threadIdx.x, ty = threadIdx.y;
+    const int tid = tx + TX * ty;
     const int x = x0 + tx, y = y0 + ty;
     const bool own = (x < nx) && (y < ny);
 
     KC<T> c;
     c.load(d, s);
 
-    auto slot5 = [](int z) { return ((z % 5) + 5) % 5; };
-    auto slot3 = [](int z) { return ((z % 3) + 3) % 3; };
+    // node-tile position of ring item r: the rows above and below the tile,
+    // then the two side columns
+    int rlx = 0, rly = 0;
+    if (tid < RING) {
+        int r = tid;
+        if (r < NW) { rlx = r; rly = 0; }
+        else if ((r -= NW) < NW) { rlx = r; rly = NH - 1; }
+        else if ((r -= NW) < TY) { rlx = 0; rly = 1 + r; }
+        else { r -= TY; rlx = NW - 1; rly = 1 + r; }
+    }
+    // global position of this thread's two node-tile items and whether they
+    // are phase nodes (1 .. N-2) / solute points (0 .. N-1)
+    const int rgx = x0 - 1 + rlx, rgy = y0 - 1 + rly;       // ring item
+    const bool ring = tid < RING;
+    const bool in_node = x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2;
+    const bool rg_node = ring && rgx >= 1 && rgx <= nx - 2 && rgy >= 1 && rgy <= ny - 2;
+    const bool in_pt = own;
+    const bool rg_pt = ring && rgx >= 0 && rgx <= nx - 1 && rgy >= 0 && rgy <= ny - 1;
+    const long long col = (long long)x + (long long)y * px;
+    const long long rg_col = (long long)rgx + (long long)rgy * px;
 
-    // issue the loads of phase plane z (in-domain elements only)
-    auto load_plane = [&](int z) {
+    // issue the loads of phase plane z into window slot sl
+    auto load_plane = [&](int z, int sl) {
         if (z < 0 || z >= nz) return;
-        T(*dst)[PW] = sm.phi[slot5(z)];
+        T(*dst)[PW] = sm.phi[sl];
         const T* src = phi_in + (long long)z * pl;
         for (int ly = ty; ly < PH; ly += TY) {
             const int gy = y0 - 2 + ly;
@@ -92,30 +126,14 @@ __global__ void __launch_bounds__(32 * TY, (TY <= 8) ? 2 : 1) k_fused(DomainDesc
         }
     };
 
-    // node-tile position of the ring item r (0 <= r < RING): the two full
-    // rows above and below the tile, then the two side columns
-    constexpr int RING = 2 * NW + 2 * TY;
-    auto ring_pos = [](int r, int& lx, int& ly) {
-        if (r < NW) { lx = r; ly = 0; return; }
-        r -= NW;
-        if (r < NW) { lx = r; ly = NH - 1; return; }
-        r -= NW;
-        if (r < TY) { lx = 0; ly = 1 + r; return; }
-        r -= TY;
-        lx = NW - 1; ly = 1 + r;
-    };
-
-    // anisotropy quantities of node plane zn over the tile + ring
-    auto node_plane = [&](int zn) {
+    // anisotropy quantities of node plane zn from phase slots (zn-1, zn, zn+1)
+    auto node_plane = [&](int zn, int sm1, int s0, int sp1, int sl) {
         if (zn < 1 || zn > nz - 2) return;
-        const T(*pm)[PW] = sm.phi[slot5(zn - 1)];
-        const T(*p0)[PW] = sm.phi[slot5(zn)];
-        const T(*pp)[PW] = sm.phi[slot5(zn + 1)];
-        const int sl = slot3(zn);
+        const T(*pm)[PW] = sm.phi[sm1];
+        const T(*p0)[PW] = sm.phi[s0];
+        const T(*pp)[PW] = sm.phi[sp1];
         auto one_node = [&](int lx, int ly) {
-            int gx = x0 - 1 + lx, gy = y0 - 1 + ly;
-            if (gx < 1 || gx > nx - 2 || gy < 1 || gy > ny - 2) return;
-            int fx = lx + 1, fy = ly + 1;   // phase-tile coordinates of the node
+            const int fx = lx + 1, fy = ly + 1;   // phase-tile coordinates of the node
             T gxv = grad<T, true>(p0[fy][fx + 1], p0[fy][fx - 1], c.dx, c.hx);
             T gyv = grad<T, true>(p0[fy + 1][fx], p0[fy - 1][fx], c.dy, c.hy);
             T gzv = grad<T, true>(pp[fy][fx], pm[fy][fx], c.dz, c.hz);
@@ -125,66 +143,87 @@ __global__ void __launch_bounds__(32 * TY, (TY <= 8) ? 2 : 1) k_fused(DomainDesc
             sm.eyz[sl][ly][lx] = n.eyz;
             sm.ezx[sl][ly][lx] = n.ezx;
         };
-        one_node(tx + 1, ty + 1);
-        if (tid < RING) {
-            int lx, ly;
-            ring_pos(tid, lx, ly);
-            one_node(lx, ly);
-        }
+        if (in_node) one_node(tx + 1, ty + 1);
+        if (rg_node) one_node(rlx, rly);
     };
 
-    // solute point quantities of plane zs over the tile + ring
-    auto sol_plane = [&](int zs) {
-        if (!SOL) return;
+    // solute point quantities of plane zs from phase slot s0 and the
+    // concentration values ci (own point) and cr (ring point) of that plane
+    auto sol_plane = [&](int zs, int s0, int sl, T ci, T cr) {
         if (zs < 0 || zs > nz - 1) return;
-        const T(*p0)[PW] = sm.phi[slot5(zs)];
-        const int sl = slot3(zs);
-        const T* cz = c_in + (long long)zs * pl;
-        auto one_point = [&](int lx, int ly) {
-            int gx = x0 - 1 + lx, gy = y0 - 1 + ly;
-            if (gx < 0 || gx > nx - 1 || gy < 0 || gy > ny - 1) return;
-            SolNode<T> n = sol_node<T, true>(p0[ly + 1][lx + 1], cz[gx + (long long)gy * px], c);
-            sm.br[sl][ly][lx] = n.br;
-            sm.mu[sl][ly][lx] = n.mu;
-        };
-        one_point(tx + 1, ty + 1);
-        if (tid < RING) {
-            int lx, ly;
-            ring_pos(tid, lx, ly);
-            one_point(lx, ly);
+        const T(*p0)[PW] = sm.phi[s0];
+        if (in_pt) {
+            SolNode<T> n = sol_node<T, true>(p0[ty + 2][tx + 2], ci, c);
+            sm.br[sl][ty + 1][tx + 1] = n.br;
+            sm.mu[sl][ty + 1][tx + 1] = n.mu;
         }
+        if (rg_pt) {
+            SolNode<T> n = sol_node<T, true>(p0[rly + 1][rlx + 1], cr, c);
+            sm.br[sl][rly][rlx] = n.br;
+            sm.mu[sl][rly][rlx] = n.mu;
+        }
+    };
+    auto load_c = [&](int zs, T& ci, T& cr) {
+        if (!SOL || zs < 0 || zs > nz - 1) return;
+        const long long zo = (long long)zs * pl;
+        if (in_pt) ci = c_in[col + zo];
+        if (rg_pt) cr = c_in[rg_col + zo];
     };
 
     // ---- prologue: planes zb-2 .. zb+2, nodes zb-1 and zb ----
-    for (int z = zb - 2; z <= zb + 2; ++z) load_plane(z);
+    int s5 = zb % 5, s3 = zb % 3;   // window slots of plane zb
+    for (int k = -2; k <= 2; ++k) load_plane(zb + k, add5(s5, (k + 5) % 5));
     cp_async_commit();
-    cp_async_wait_all();
-    __syncthreads();
-    node_plane(zb - 1);
-    node_plane(zb);
-    sol_plane(zb - 1);
-    sol_plane(zb);
+    T cpi = 0, cpr = 0, cqi = 0, cqr = 0;   // c of solute planes z+1 (p) and z+2 (q)
+    if (SOL) {
+        T ai = 0, ar = 0, bi = 0, br_ = 0;
+        load_c(zb - 1, ai, ar);
+        load_c(zb, bi, br_);
+        load_c(zb + 1, cpi, cpr);
+        cp_async_wait_all();
+        __syncthreads();
+        sol_plane(zb - 1, add5(s5, 4), add3(s3, 2), ai, ar);
+        sol_plane(zb, s5, s3, bi, br_);
+    } else {
+        cp_async_wait_all();
+        __syncthreads();
+    }
+    node_plane(zb - 1, add5(s5, 3), add5(s5, 4), s5, add3(s3, 2));
+    node_plane(zb, add5(s5, 4), s5, add5(s5, 1), s3);
 
     const int fx = tx + 2, fy = ty + 2;   // own cell in the phase tile
     const int nlx = tx + 1, nly = ty + 1; // own cell in the node tile
     const bool xs_src = x >= 1 && x <= nx - 2, ys_src = y >= 1 && y <= ny - 2;
     const bool xs_int = x >= 2 && x <= nx - 3, ys_int = y >= 2 && y <= ny - 3;
+    const bool single_xy = x >= 3 && x <= nx - 4 && y >= 3 && y <= ny - 4;
     int xl = 0, xh = -1, yl = 0, yh = -1;
     if (own && xs_src) fpre_range(x, nx, &xl, &xh);
     if (own && ys_src) fpre_range(y, ny, &yl, &yh);
+    long long zoff = (long long)zb * pl;
 
-    for (int z = zb; z < ze; ++z) {
-        node_plane(z + 1);
-        sol_plane(z + 1);
+    for (int z = zb; z < ze; ++z, zoff += pl) {
+        const long long id = col + zoff;
+        // centre values from global memory, consumed after the node pass
+        T cpp = 0, dppv = 0, told = 0;
+        if (own) {
+            cpp = c_in[id];
+            if (HEAT) {
+                dppv = dpp[id];
+                told = T_old[id];
+            }
+        }
+        if (SOL) load_c(z + 2, cqi, cqr);
+        node_plane(z + 1, s5, add5(s5, 1), add5(s5, 2), add3(s3, 1));
+        if (SOL) sol_plane(z + 1, add5(s5, 1), add3(s3, 1), cpi, cpr);
         __syncthreads();
-        load_plane(z + 3);
+        load_plane(z + 3, add5(s5, 3));
         cp_async_commit();
 
         if (own) {
-            const long long id = (long long)x + (long long)y * px + (long long)z * pl;
-            const T(*pm)[PW] = sm.phi[slot5(z - 1)];
-            const T(*p0)[PW] = sm.phi[slot5(z)];
-            const T(*pp)[PW] = sm.phi[slot5(z + 1)];
+            const T(*pm)[PW] = sm.phi[add5(s5, 4)];
+            const T(*p0)[PW] = sm.phi[s5];
+            const T(*pp)[PW] = sm.phi[add5(s5, 1)];
+            const int n0 = s3, np1 = add3(s3, 1), nm1 = add3(s3, 2);
             const T PPc = p0[fy][fx];
             const bool zin = z >= 1 && z <= nz - 2;
 
@@ -196,18 +235,16 @@ __global__ void __launch_bounds__(32 * TY, (TY <= 8) ? 2 : 1) k_fused(DomainDesc
                         TE = T_old[id + 1]; TW = T_old[id - 1]; TN = T_old[id + px]; TS = T_old[id - px];
                         TT = T_old[id + pl]; TB = T_old[id - pl];
                     }
-                    T_new[id] = heat_new<T>(PPc, dpp[id], TE, TW, TN, TS, TT, TB, c);
+                    T_new[id] = heat_new<T>(PPc, dppv, TE, TW, TN, TS, TT, TB, c);
                 } else {
-                    T_new[id] = T_old[id];
+                    T_new[id] = told;
                 }
             }
 
             // ---- phase sweep ----
-            const bool src = xs_src && ys_src && zin;
-            if (src) {
+            if (xs_src && ys_src && zin) {
                 T U;
-                const bool interior = xs_int && ys_int && z >= 2 && z <= nz - 3;
-                if (interior) {
+                if (xs_int && ys_int && z >= 2 && z <= nz - 3) {
                     Nbr<T> nb;
                     nb.PP = PPc;
                     nb.PN = p0[fy + 1][fx]; nb.PS = p0[fy - 1][fx];
@@ -219,62 +256,66 @@ __global__ void __launch_bounds__(32 * TY, (TY <= 8) ? 2 : 1) k_fused(DomainDesc
                     nb.PST = pp[fy - 1][fx]; nb.PSB = pm[fy - 1][fx];
                     nb.PET = pp[fy][fx + 1]; nb.PEB = pm[fy][fx + 1];
                     nb.PWT = pp[fy][fx - 1]; nb.PWB = pm[fy][fx - 1];
-                    const int s0 = slot3(z), sp = slot3(z + 1), sm1 = slot3(z - 1);
                     Node<T> E, W, N, S, Tt, B;
-                    E.eps = sm.eps[s0][nly][nlx + 1]; E.exy = sm.exy[s0][nly][nlx + 1]; E.ezx = sm.ezx[s0][nly][nlx + 1];
-                    W.eps = sm.eps[s0][nly][nlx - 1]; W.exy = sm.exy[s0][nly][nlx - 1]; W.ezx = sm.ezx[s0][nly][nlx - 1];
-                    N.eps = sm.eps[s0][nly + 1][nlx]; N.exy = sm.exy[s0][nly + 1][nlx]; N.eyz = sm.eyz[s0][nly + 1][nlx];
-                    S.eps = sm.eps[s0][nly - 1][nlx]; S.exy = sm.exy[s0][nly - 1][nlx]; S.eyz = sm.eyz[s0][nly - 1][nlx];
-                    Tt.eps = sm.eps[sp][nly][nlx]; Tt.eyz = sm.eyz[sp][nly][nlx]; Tt.ezx = sm.ezx[sp][nly][nlx];
-                    B.eps = sm.eps[sm1][nly][nlx]; B.eyz = sm.eyz[sm1][nly][nlx]; B.ezx = sm.ezx[sm1][nly][nlx];
+                    E.eps = sm.eps[n0][nly][nlx + 1]; E.exy = sm.exy[n0][nly][nlx + 1]; E.ezx = sm.ezx[n0][nly][nlx + 1];
+                    W.eps = sm.eps[n0][nly][nlx - 1]; W.exy = sm.exy[n0][nly][nlx - 1]; W.ezx = sm.ezx[n0][nly][nlx - 1];
+                    N.eps = sm.eps[n0][nly + 1][nlx]; N.exy = sm.exy[n0][nly + 1][nlx]; N.eyz = sm.eyz[n0][nly + 1][nlx];
+                    S.eps = sm.eps[n0][nly - 1][nlx]; S.exy = sm.exy[n0][nly - 1][nlx]; S.eyz = sm.eyz[n0][nly - 1][nlx];
+                    Tt.eps = sm.eps[np1][nly][nlx]; Tt.eyz = sm.eyz[np1][nly][nlx]; Tt.ezx = sm.ezx[np1][nly][nlx];
+                    B.eps = sm.eps[nm1][nly][nlx]; B.eyz = sm.eyz[nm1][nly][nlx]; B.ezx = sm.ezx[nm1][nly][nlx];
                     E.eyz = W.eyz = N.ezx = S.ezx = Tt.exy = B.exy = (T)0;   // unused by the body
                     float ran = phase_ran(c.rt, x + 1, y + 1, z + 1, c.it);
-                    T ppn = phase_ppnew<T, true>(nb, E, W, N, S, Tt, B, c_in[id], ran, c);
+                    T ppn = phase_ppnew<T, true>(nb, E, W, N, S, Tt, B, cpp, ran, c);
                     if (DPPW) dpp[id] = ppn - PPc;
                     U = clamp01(ppn);
                 } else {
                     U = PPc;
                 }
-                int zl, zh;
-                fpre_range(z, nz, &zl, &zh);
-                for (int zz = zl; zz <= zh; ++zz)
-                    for (int yy = yl; yy <= yh; ++yy)
-                        for (int xx = xl; xx <= xh; ++xx)
-                            phi_out[(long long)xx + (long long)yy * px + (long long)zz * pl] = U;
+                if (single_xy && z >= 3 && z <= nz - 4) {
+                    phi_out[id] = U;   // its only preimage is itself
+                } else {
+                    int zl, zh;
+                    fpre_range(z, nz, &zl, &zh);
+                    for (int zz = zl; zz <= zh; ++zz)
+                        for (int yy = yl; yy <= yh; ++yy)
+                            for (int xx = xl; xx <= xh; ++xx)
+                                phi_out[(long long)xx + (long long)yy * px + (long long)zz * pl] = U;
+                }
             }
 
             // ---- solute ----
             if (SOL) {
-                const bool xin = xs_src, yin = ys_src;
-                const bool inner = xin && yin && zin;
+                const bool inner = xs_src && ys_src && zin;
                 const bool feeds = inner || z == 1 || z == nz - 2 || (zin && (x == 1 || x == nx - 2));
                 if (feeds) {
                     T Uc;
                     if (inner) {
-                        const int s0 = slot3(z), sp = slot3(z + 1), sm1 = slot3(z - 1);
-                        SolNode<T> nP{sm.br[s0][nly][nlx], sm.mu[s0][nly][nlx]};
-                        SolNode<T> nE{sm.br[s0][nly][nlx + 1], sm.mu[s0][nly][nlx + 1]};
-                        SolNode<T> nW{sm.br[s0][nly][nlx - 1], sm.mu[s0][nly][nlx - 1]};
-                        SolNode<T> nN{sm.br[s0][nly + 1][nlx], sm.mu[s0][nly + 1][nlx]};
-                        SolNode<T> nS{sm.br[s0][nly - 1][nlx], sm.mu[s0][nly - 1][nlx]};
-                        SolNode<T> nT{sm.br[sp][nly][nlx], sm.mu[sp][nly][nlx]};
-                        SolNode<T> nB{sm.br[sm1][nly][nlx], sm.mu[sm1][nly][nlx]};
-                        Uc = conc_new<T, true>(PPc, c_in[id], nP, nE, nW, nN, nS, nT, nB, c);
+                        SolNode<T> nP{sm.br[n0][nly][nlx], sm.mu[n0][nly][nlx]};
+                        SolNode<T> nE{sm.br[n0][nly][nlx + 1], sm.mu[n0][nly][nlx + 1]};
+                        SolNode<T> nW{sm.br[n0][nly][nlx - 1], sm.mu[n0][nly][nlx - 1]};
+                        SolNode<T> nN{sm.br[n0][nly + 1][nlx], sm.mu[n0][nly + 1][nlx]};
+                        SolNode<T> nS{sm.br[n0][nly - 1][nlx], sm.mu[n0][nly - 1][nlx]};
+                        SolNode<T> nT{sm.br[np1][nly][nlx], sm.mu[np1][nly][nlx]};
+                        SolNode<T> nB{sm.br[nm1][nly][nlx], sm.mu[nm1][nly][nlx]};
+                        Uc = conc_new<T, true>(PPc, cpp, nP, nE, nW, nN, nS, nT, nB, c);
                         c_out[id] = Uc;
                     } else {
-                        Uc = c_in[id];
+                        Uc = cpp;
                     }
                     if (z == 1) c_out[id - pl] = Uc;
                     if (z == nz - 2) c_out[id + pl] = Uc;
                     if (zin && x == 1) c_out[id - 1] = Uc;
                     if (zin && x == nx - 2) c_out[id + 1] = Uc;
-                    if (zin && xin && y == 1) c_out[id - px] = Uc;
-                    if (zin && xin && y == ny - 2) c_out[id + px] = Uc;
+                    if (zin && xs_src && y == 1) c_out[id - px] = Uc;
+                    if (zin && xs_src && y == ny - 2) c_out[id + px] = Uc;
                 }
             }
         }
+        if (SOL) { cpi = cqi; cpr = cqr; }
         cp_async_wait_all();
         __syncthreads();
+        s5 = add5(s5, 1);
+        s3 = add3(s3, 1);
     }
 }
 
