@@ -203,6 +203,14 @@ int pf_diagnosticos_noalloc(const void* phase_field, const void* conc_soluto, in
                             int pitch, int precision, double dx, double dy, double dz, double E0,
                             double W0, void* stream, double out[5]);
 
+/* Seeded synthetic initial state written on the device into the old fields
+   and DPP (the reference fills its fields on the host, entrada.f90:226-262):
+   a solid slab k <= 4 carrying hemispherical bumps of radius 3 cells at the
+   1-based (i, j) centres sites[2*b], sites[2*b+1]; phi = (1-tanh(2d/w))/2
+   with d the signed distance to slab U bumps and w = Thin_Interface cells;
+   c = C0 (1 - (1 - Ke) phi); T = T0; DPP = 0.  At most 4096 bumps.        */
+int pf_init_seeded(pf_ctx* ctx, int n_bumps, const double* sites);
+
 /* ---- fused step ------------------------------------------------------- */
 /* Runs n_steps whole iterations of principal.f90:93-226 (temperatura, TP
    ramp, n_varreduras sweeps, solute, auxiliar, swap) with the fused
@@ -211,6 +219,41 @@ int pf_diagnosticos_noalloc(const void* phase_field, const void* conc_soluto, in
 int pf_step(pf_ctx* ctx, int n_steps);
 /* Same, and also fills out[5] with the diagnostics of the final state.    */
 int pf_step_diag(pf_ctx* ctx, int n_steps, double out[5]);
+
+/* ---- batches of independent domains ---------------------------------- */
+/* Many domains of one precision, each with its own grid, deck and step
+   count, advanced together: one persistent launch per pass over a work list
+   of (domain, tile) items, K steps per captured CUDA graph.  Domains join
+   (pf_batch_add) and leave (pf_batch_remove) between pf_batch_step calls
+   under a device-memory budget; each keeps the reference's per-domain step
+   semantics of pf_step, and its results are the same bits as pf_step's on
+   the same domain.  All domains of a batch use the same n_varreduras (1/2). */
+typedef struct pf_batch pf_batch;
+int pf_batch_create(int precision, long long budget_bytes, int max_domains, pf_batch** out);
+int pf_batch_destroy(pf_batch* b);
+int pf_batch_set_stream(pf_batch* b, void* stream);
+long long pf_batch_bytes_used(const pf_batch* b);
+int pf_batch_count(const pf_batch* b);
+/* PF_E_NOMEM when the domain does not fit the budget or no slot is free    */
+int pf_batch_add(pf_batch* b, const pf_grid* g, const pf_params* p, int* slot);
+int pf_batch_remove(pf_batch* b, int slot);
+int pf_batch_upload(pf_batch* b, int slot, int field, const double* host);
+int pf_batch_download(pf_batch* b, int slot, int field, double* host);
+int pf_batch_init_seeded(pf_batch* b, int slot, int n_bumps, const double* sites);
+/* the slot stops advancing once it has completed target_it steps (0: never) */
+int pf_batch_set_target(pf_batch* b, int slot, long long target_it);
+int pf_batch_get_state(const pf_batch* b, int slot, pf_state* out);
+/* advance every active slot by up to n_steps steps                        */
+int pf_batch_step(pf_batch* b, int n_steps);
+/* device milliseconds of the last pf_batch_step call (all its graphs)      */
+double pf_batch_last_ms(const pf_batch* b);
+int pf_batch_set_tile(pf_batch* b, int tile_y, int zchunk);
+/* Autotuner: times every tile height (4, 8, 16) x z-chunk (16, 32, 64, 128)
+   on real steps (the results do not depend on the tile shape; each candidate
+   advances the batch by 1 + steps_per_candidate steps), keeps the fastest
+   and caches it per shape class (precision, median column size and depth) */
+int pf_batch_autotune(pf_batch* b, int steps_per_candidate, int* tile_y, int* zchunk, double* ms_per_step);
+int pf_batch_diagnosticos(pf_batch* b, int slot, double out[5]);
 
 #ifdef __cplusplus
 }

@@ -15,6 +15,8 @@
 #include "../../include/pf3d.h"
 #include "pf3d_launch.h"
 #include "pf3d_scalar.h"
+#include "pf3d_hostdesc.h"
+#include "pf3d_init.cuh"
 
 using namespace pf3d;
 
@@ -80,70 +82,6 @@ static int cuda_check(pf_ctx* c, cudaError_t e, const char* what)
     } while (0)
 
 static inline bool is64(const pf_ctx* c) { return c->prec == PF_FP64; }
-
-static void fill_desc(const pf_grid& g, const pf_params& p, const pf_derived& dv, int px, DomainDesc& d)
-{
-    std::memset(&d, 0, sizeof(d));
-    d.nx = g.nx; d.ny = g.ny; d.nz = g.nz;
-    d.px = px;
-    d.plane = (long long)px * g.ny;
-    d.dx = g.dx; d.dy = g.dy; d.dz = g.dz;
-    d.E0 = dv.E0; d.W0 = dv.W0; d.DE = p.DELTA_EPSLON;
-    d.K_aniso = 16.0 * dv.E0 * p.DELTA_EPSLON;       // phase_body.inc:49
-    d.AAA = dv.AAA;
-    d.Ke = (double)p.Ke;
-    d.D_liq = p.D_liq; d.D_sol = p.D_sol;
-    d.dt = dv.DELTA_T;
-    d.dH_cp = p.delta_H / p.Cp_s;                     // temp_body.inc:36, cp = cp_s
-    d.Ddt = p.D * dv.DELTA_T;                         // temp_body.inc:41
-    d.cxy = 0.25 / (g.dx * g.dy);
-    d.cyz = 0.25 / (g.dy * g.dz);
-    d.czx = 0.25 / (g.dz * g.dx);
-    d.dx2 = g.dx * g.dx; d.dy2 = g.dy * g.dy; d.dz2 = g.dz * g.dz;
-    d.InvDX = 1.0 / (g.dx * g.dx); d.InvDY = 1.0 / (g.dy * g.dy); d.InvDZ = 1.0 / (g.dz * g.dz);
-    d.hx = 0.5 / g.dx; d.hy = 0.5 / g.dy; d.hz = 0.5 / g.dz;
-    d.rdx2 = 1.0 / (g.dx * g.dx); d.rdy2 = 1.0 / (g.dy * g.dy); d.rdz2 = 1.0 / (g.dz * g.dz);
-    d.AAA16 = dv.AAA * 16.0;
-    d.omKe = 1.0 - (double)p.Ke;
-    d.dtIX = dv.DELTA_T * d.InvDX; d.dtIY = dv.DELTA_T * d.InvDY; d.dtIZ = dv.DELTA_T * d.InvDZ;
-    d.hq = p.h_quintico;
-    d.rt = p.ruido_tipo;
-    d.do_heat_lap = (p.D != 0.0) ? 1 : 0;
-}
-
-static StepArgs make_step_args(const pf_ctx* c, int it, double TP_heat, double TP, double M0)
-{
-    StepArgs s;
-    std::memset(&s, 0, sizeof(s));
-    double Cs, Cl;
-    equilibrium(c->p, TP, &Cs, &Cl);
-    s.it = it;
-    s.TP_heat = TP_heat;
-    s.TP = TP;
-    s.M0dt = M0 * c->dv.DELTA_T;
-    s.RTV = c->p.R * TP / c->p.Vm;
-    s.omCs = 1.0 - Cs;
-    s.omCl = 1.0 - Cl;
-    s.Lc = std::log(s.omCs / s.omCl);
-    return s;
-}
-
-static int validate(const pf_grid* g, const pf_params* p, int precision, std::string& why)
-{
-    if (!g || !p) { why = "null grid or params"; return PF_E_ARG; }
-    if (g->nx < 5 || g->ny < 5 || g->nz < 5) { why = "every grid dimension must be >= 5"; return PF_E_ARG; }
-    if (!(g->dx > 0) || !(g->dy > 0) || !(g->dz > 0)) { why = "grid spacings must be > 0"; return PF_E_ARG; }
-    if (precision != PF_FP64 && precision != PF_FP32) { why = "precision must be 64 or 32"; return PF_E_ARG; }
-    if (!(p->D_liq > 0) || !(p->Cp_s != 0) || !(p->Me != 0) || !(p->Vm != 0)) { why = "D_liq, Cp_s, Me, Vm must be nonzero"; return PF_E_ARG; }
-    if (p->n_varreduras < 1) { why = "n_varreduras must be >= 1"; return PF_E_ARG; }
-    if (p->h_quintico != 0 && p->h_quintico != 1) { why = "h_quintico must be 0 or 1"; return PF_E_ARG; }
-    if (p->ruido_tipo < 0 || p->ruido_tipo > 2) { why = "ruido_tipo must be 0, 1 or 2"; return PF_E_ARG; }
-    if (p->bc != PF_BC_REFERENCE) { why = "only the reference boundary treatment is available"; return PF_E_ARG; }
-    return PF_OK;
-}
-
-static size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
-static int pitch_of(int nx) { return (int)round_up((size_t)nx, 32); }
 
 extern "C" {
 
@@ -401,7 +339,7 @@ static Fields fields_of(const pf_ctx* ctx)
 int pf_temperatura(pf_ctx* ctx, double TP)
 {
     if (!ctx) return PF_E_ARG;
-    StepArgs s = make_step_args(ctx, ctx->st.it, TP, TP, ctx->st.M0);
+    StepArgs s = make_step_args(ctx->p, ctx->dv, ctx->st.it, TP, TP, ctx->st.M0);
     Fields f = fields_of(ctx);
     CK(is64(ctx) ? launch_heat<double>(ctx->dd, s, f, ctx->stream) : launch_heat<float>(ctx->dd, s, f, ctx->stream),
        "temperatura");
@@ -411,7 +349,7 @@ int pf_temperatura(pf_ctx* ctx, double TP)
 int pf_equacao_campo_fase(pf_ctx* ctx, int it, double TP, double M0, double* Cs_eq, double* Cl_eq)
 {
     if (!ctx) return PF_E_ARG;
-    StepArgs s = make_step_args(ctx, it, TP, TP, M0);
+    StepArgs s = make_step_args(ctx->p, ctx->dv, it, TP, TP, M0);
     double Cs, Cl;
     equilibrium(ctx->p, TP, &Cs, &Cl);
     ctx->st.Cs_eq = Cs;
@@ -437,7 +375,7 @@ int pf_copy_phase_new_to_old(pf_ctx* ctx)
 int pf_concentracao_soluto(pf_ctx* ctx)
 {
     if (!ctx) return PF_E_ARG;
-    StepArgs s = make_step_args(ctx, ctx->st.it, ctx->st.TP, ctx->st.TP, ctx->st.M0);
+    StepArgs s = make_step_args(ctx->p, ctx->dv, ctx->st.it, ctx->st.TP, ctx->st.TP, ctx->st.M0);
     Fields f = fields_of(ctx);
     if (is64(ctx)) {
         CK(launch_solute<double>(ctx->dd, s, f.phi_old, f.c_old, f.c_new, ctx->stream), "concentracao_soluto");
@@ -498,7 +436,7 @@ static int one_step(pf_ctx* ctx)
     ctx->st.time = (float)(dt + (double)ctx->st.time);          // principal.f90:96 (REAL(4) time)
     const double TP_heat = ctx->st.TP;                          // temperatura sees the previous TP
     const double TP = step_tp(p, dt, it, ctx->st.TP);           // principal.f90:104
-    const StepArgs s = make_step_args(ctx, it, TP_heat, TP, ctx->st.M0);
+    const StepArgs s = make_step_args(ctx->p, ctx->dv, it, TP_heat, TP, ctx->st.M0);
     const int nsw = p.n_varreduras;
     void* A = ctx->fld[PF_PHASE_OLD];
     void* B = ctx->fld[PF_PHASE_NEW];
@@ -595,6 +533,32 @@ int pf_step_diag(pf_ctx* ctx, int n_steps, double out[5])
     if (rc) return rc;
     // after the exchange the final state sits in the "old" buffers
     return run_diag(ctx, ctx->fld[PF_PHASE_OLD], ctx->fld[PF_CONC_OLD], out);
+}
+
+int pf_init_seeded(pf_ctx* ctx, int n_bumps, const double* sites)
+{
+    if (!ctx || n_bumps < 0 || n_bumps > 4096 || (n_bumps > 0 && !sites))
+        return ctx_err(ctx, PF_E_ARG, "pf_init_seeded: bad argument (at most 4096 bumps)");
+    int rc = ensure_stage(ctx);
+    if (rc) return rc;
+    InitArgs a;
+    a.n_bumps = n_bumps;
+    a.slab_top = 4.5;
+    a.bump_r = 3.0;
+    a.width = ctx->p.Thin_Interface;
+    a.kmax = std::min(ctx->g.nz, (int)(a.slab_top + a.bump_r + 20.0 * a.width / 2.0) + 2);
+    a.C0 = ctx->p.C0;
+    a.Ke = (double)ctx->p.Ke;
+    a.T0 = ctx->p.T0;
+    if (n_bumps)
+        CK(cudaMemcpyAsync(ctx->d_stage, sites, 2 * n_bumps * sizeof(double), cudaMemcpyHostToDevice, ctx->stream),
+           "bump sites");
+    Fields f = fields_of(ctx);
+    CK(is64(ctx) ? launch_init_seeded<double>(ctx->dd, a, ctx->d_stage, f.phi_old, f.c_old, f.T_old, f.dpp, ctx->stream)
+                 : launch_init_seeded<float>(ctx->dd, a, ctx->d_stage, f.phi_old, f.c_old, f.T_old, f.dpp, ctx->stream),
+       "pf_init_seeded");
+    CK(cudaStreamSynchronize(ctx->stream), "pf_init_seeded sync");
+    return PF_OK;
 }
 
 int pf_kernel_times(pf_ctx* ctx, long* n_first, double* ms_first, long* n_last, double* ms_last, int reset)

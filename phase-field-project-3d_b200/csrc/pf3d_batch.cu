@@ -1,0 +1,624 @@
+// pf3d_batch.cu -- many independent domains stepped together (C-ABI pf_batch_*).
+//
+// A batch holds up to max_domains domains of one precision, each with its own
+// grid, deck and step count, under a device-memory budget.  All active
+// domains advance together: one persistent kernel per pass walks a work list
+// of (domain, tile) items, and K steps are captured once in a CUDA graph.
+// Everything that changes between launches lives in device tables the host
+// rewrites in stream order:
+//   doms   : descriptor and buffer pointers of every slot,
+//   items  : the work list (rebuilt when membership or the tile shape changes),
+//   steps  : per step and slot the step scalars (TP, M0, it, ...), whether the
+//            slot advances in that step, and which buffer holds the old field.
+// So domains join and leave between graph launches without recapture
+// (continuous batching), and a slot that reaches its target step count stops
+// while the others go on.  Per-domain results are the same bits as stepping
+// that domain alone: the tile function is the one of pf_step and no value
+// depends on the tile shape, the z-chunk or the other domains.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+#include "../../include/pf3d.h"
+#include "pf3d_hostdesc.h"
+#include "pf3d_init.cuh"
+
+using namespace pf3d;
+
+namespace pf3d {
+int set_last_error_global(int code, const std::string& msg);
+}
+
+namespace {
+
+constexpr int kGraphSteps = 8;   // steps per captured graph
+
+struct Slot {
+    bool used = false;
+    pf_grid g{};
+    pf_params p{};
+    pf_derived dv{};
+    pf_state st{};
+    long long target = 0;     // stop after this step (0 = no limit)
+    int qphi = 0, qc = 0, qT = 0;
+    void* mem = nullptr;
+    size_t bytes = 0;
+    BatchDomain bd{};
+};
+
+// autotuner cache: shape class -> (tile_y, zchunk)
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int>, std::pair<int, int>> g_tune_cache;
+
+}  // namespace
+
+struct pf_batch {
+    int prec = 64;
+    size_t es = 8;
+    long long budget = 0, used_bytes = 0;
+    int max_domains = 0;
+    int nsw = 0;                       // sweeps per step shared by all slots (1 or 2)
+    std::vector<Slot> slots;
+    BatchDomain* d_doms = nullptr;
+    BatchStep* d_steps = nullptr;      // kGraphSteps x max_domains
+    BatchStep* h_steps[2] = {nullptr, nullptr};
+    cudaEvent_t h_ev[2] = {nullptr, nullptr};
+    int h_cur = 0;
+    BatchItem* d_items = nullptr;
+    int item_cap = 0;
+    int* d_nitems = nullptr;
+    bool items_dirty = true;
+    double* d_part = nullptr;          // diagnostics partials (592 x 8) + result
+    double* h_out = nullptr;
+    double* d_sites = nullptr;         // bump sites for device initialisation
+    int tile_y = 8, zchunk = 64, grid = 0;
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_ty = 0, graph_zc = 0, graph_grid = 0, graph_nsw = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0.0;
+    long long last_steps = 0;
+    std::string err;
+};
+
+static int berr(pf_batch* b, int code, const std::string& msg)
+{
+    if (b) b->err = msg;
+    return set_last_error_global(code, msg);
+}
+
+#define BCK(call, what)                                                                  \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) return berr(b, PF_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+static bool b64(const pf_batch* b) { return b->prec == PF_FP64; }
+
+static int rebuild_items(pf_batch* b)
+{
+    std::vector<BatchItem> items;
+    // largest domains first: their items are the longest-running
+    std::vector<int> order;
+    for (int s = 0; s < (int)b->slots.size(); ++s)
+        if (b->slots[s].used) order.push_back(s);
+    std::sort(order.begin(), order.end(), [&](int a, int c) {
+        const pf_grid& ga = b->slots[a].g;
+        const pf_grid& gc = b->slots[c].g;
+        return (long long)ga.nz > (long long)gc.nz || (ga.nz == gc.nz && a < c);
+    });
+    for (int s : order) {
+        const pf_grid& g = b->slots[s].g;
+        const int nbx = (g.nx + 31) / 32, nby = (g.ny + b->tile_y - 1) / b->tile_y;
+        const int nbz = (g.nz + b->zchunk - 1) / b->zchunk;
+        for (int bz = 0; bz < nbz; ++bz)
+            for (int by = 0; by < nby; ++by)
+                for (int bx = 0; bx < nbx; ++bx) items.push_back(BatchItem{s, bx, by, bz});
+    }
+    const int n = (int)items.size();
+    if (n > b->item_cap) {
+        BCK(cudaStreamSynchronize(b->stream), "work list resize");
+        if (b->d_items) cudaFree(b->d_items);
+        if (b->graph) {   // the captured launches point at the old list
+            cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+        }
+        b->item_cap = std::max(n, 2 * b->item_cap);
+        BCK(cudaMalloc(&b->d_items, (size_t)b->item_cap * sizeof(BatchItem)), "work list");
+    }
+    if (n) BCK(cudaMemcpyAsync(b->d_items, items.data(), n * sizeof(BatchItem), cudaMemcpyHostToDevice, b->stream),
+               "work list upload");
+    BCK(cudaMemcpyAsync(b->d_nitems, &n, sizeof(int), cudaMemcpyHostToDevice, b->stream), "work list size");
+    BCK(cudaStreamSynchronize(b->stream), "work list sync");   // the host vector goes out of scope
+    b->items_dirty = false;
+    return PF_OK;
+}
+
+static int capture_graph(pf_batch* b)
+{
+    if (b->graph && b->graph_ty == b->tile_y && b->graph_zc == b->zchunk && b->graph_grid == b->grid &&
+        b->graph_nsw == b->nsw)
+        return PF_OK;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    cudaStream_t cs;
+    BCK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "capture stream");
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        for (int k = 0; k < kGraphSteps && e == cudaSuccess; ++k) {
+            const BatchStep* st = b->d_steps + (size_t)k * b->max_domains;
+            const bool one = b->nsw == 1;
+            e = b64(b) ? launch_fused_batch<double>(b->d_doms, st, b->d_items, b->d_nitems, 0, one, b->tile_y, b->zchunk,
+                                                    b->grid, cs)
+                       : launch_fused_batch<float>(b->d_doms, st, b->d_items, b->d_nitems, 0, one, b->tile_y, b->zchunk,
+                                                   b->grid, cs);
+            if (e == cudaSuccess && !one)
+                e = b64(b) ? launch_fused_batch<double>(b->d_doms, st, b->d_items, b->d_nitems, 1, false, b->tile_y,
+                                                        b->zchunk, b->grid, cs)
+                           : launch_fused_batch<float>(b->d_doms, st, b->d_items, b->d_nitems, 1, false, b->tile_y,
+                                                       b->zchunk, b->grid, cs);
+        }
+        cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+        if (e == cudaSuccess) e = e2;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess) return berr(b, PF_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    b->graph_ty = b->tile_y;
+    b->graph_zc = b->zchunk;
+    b->graph_grid = b->grid;
+    b->graph_nsw = b->nsw;
+    return PF_OK;
+}
+
+static int set_grid(pf_batch* b)
+{
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int per = b64(b) ? batch_blocks_per_sm<double>(b->tile_y) : batch_blocks_per_sm<float>(b->tile_y);
+    b->grid = std::max(1, nsm) * per;
+    return PF_OK;
+}
+
+// Fills step table rows for up to kGraphSteps steps; returns how many steps
+// any slot advances.  Advances each slot's host state like pf_step does.
+static int fill_steps(pf_batch* b, BatchStep* rows, int nsteps)
+{
+    int advanced = 0;
+    std::memset(rows, 0, sizeof(BatchStep) * (size_t)kGraphSteps * b->max_domains);
+    for (int k = 0; k < kGraphSteps; ++k) {
+        for (int sidx = 0; sidx < (int)b->slots.size(); ++sidx) {
+            Slot& sl = b->slots[sidx];
+            BatchStep& r = rows[(size_t)k * b->max_domains + sidx];
+            r.active = 0;
+            if (!sl.used || k >= nsteps) continue;
+            if (sl.target > 0 && sl.st.it >= sl.target) continue;
+            const pf_params& p = sl.p;
+            const int it = sl.st.it + 1;
+            const double dt = sl.dv.DELTA_T;
+            const double TP_heat = sl.st.TP;
+            const double TP = step_tp(p, dt, it, sl.st.TP);
+            r.s = make_step_args(p, sl.dv, it, TP_heat, TP, sl.st.M0);
+            r.active = 1;
+            r.q_phi = sl.qphi;
+            r.q_c = sl.qc;
+            r.q_T = sl.qT;
+            // host state after the step (principal.f90:96-157 and the swap)
+            sl.st.time = (float)(dt + (double)sl.st.time);
+            if (b->nsw == 1) sl.qphi ^= 1;   // the new phase lands in the other buffer
+            sl.qc ^= 1;
+            sl.qT ^= 1;
+            double Cs, Cl, M0n;
+            equilibrium(p, TP, &Cs, &Cl);
+            pf_auxiliar_scalar(&p, sl.dv.E0, sl.dv.W0, TP, Cs, Cl, &M0n);
+            sl.st.M0 = M0n;
+            sl.st.TP = TP;
+            sl.st.Cs_eq = Cs;
+            sl.st.Cl_eq = Cl;
+            sl.st.it = it;
+            advanced = std::max(advanced, k + 1);
+        }
+    }
+    return advanced;
+}
+
+extern "C" {
+
+int pf_batch_create(int precision, long long budget_bytes, int max_domains, pf_batch** out)
+{
+    if (!out) return set_last_error_global(PF_E_ARG, "pf_batch_create: out is null");
+    *out = nullptr;
+    if ((precision != PF_FP64 && precision != PF_FP32) || max_domains < 1 || max_domains > 65536 || budget_bytes < 0)
+        return set_last_error_global(PF_E_ARG, "pf_batch_create: bad precision, max_domains or budget");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return set_last_error_global(PF_E_NODEV, "no CUDA device visible");
+    }
+    pf_batch* b = new pf_batch();
+    b->prec = precision;
+    b->es = precision == PF_FP32 ? 4 : 8;
+    b->budget = budget_bytes;
+    b->max_domains = max_domains;
+    b->slots.resize(max_domains);
+    cudaError_t e = cudaSuccess;
+    const size_t step_bytes = sizeof(BatchStep) * (size_t)kGraphSteps * max_domains;
+    if ((e = cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_doms, sizeof(BatchDomain) * (size_t)max_domains)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_steps, step_bytes)) != cudaSuccess ||
+        (e = cudaMallocHost(&b->h_steps[0], step_bytes)) != cudaSuccess ||
+        (e = cudaMallocHost(&b->h_steps[1], step_bytes)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_nitems, sizeof(int))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_part, (592 * 8 + 8) * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_sites, 2 * 4096 * sizeof(double))) != cudaSuccess ||
+        (e = cudaMallocHost(&b->h_out, 8 * sizeof(double))) != cudaSuccess ||
+        (e = cudaEventCreate(&b->h_ev[0])) != cudaSuccess || (e = cudaEventCreate(&b->h_ev[1])) != cudaSuccess ||
+        (e = cudaEventCreate(&b->ev0)) != cudaSuccess || (e = cudaEventCreate(&b->ev1)) != cudaSuccess) {
+        pf_batch_destroy(b);
+        return set_last_error_global(PF_E_CUDA, std::string("pf_batch_create: ") + cudaGetErrorString(e));
+    }
+    b->stream = b->own_stream;
+    cudaMemset(b->d_steps, 0, step_bytes);
+    cudaMemset(b->d_nitems, 0, sizeof(int));
+    set_grid(b);
+    *out = b;
+    return PF_OK;
+}
+
+int pf_batch_destroy(pf_batch* b)
+{
+    if (!b) return PF_OK;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (auto& s : b->slots)
+        if (s.mem) cudaFree(s.mem);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    cudaFree(b->d_doms);
+    cudaFree(b->d_steps);
+    cudaFreeHost(b->h_steps[0]);
+    cudaFreeHost(b->h_steps[1]);
+    cudaFree(b->d_items);
+    cudaFree(b->d_nitems);
+    cudaFree(b->d_part);
+    cudaFree(b->d_sites);
+    cudaFreeHost(b->h_out);
+    for (cudaEvent_t ev : {b->h_ev[0], b->h_ev[1], b->ev0, b->ev1})
+        if (ev) cudaEventDestroy(ev);
+    if (b->own_stream) cudaStreamDestroy(b->own_stream);
+    delete b;
+    return PF_OK;
+}
+
+int pf_batch_set_stream(pf_batch* b, void* stream)
+{
+    if (!b) return PF_E_ARG;
+    b->stream = stream ? (cudaStream_t)stream : b->own_stream;
+    return PF_OK;
+}
+
+long long pf_batch_bytes_used(const pf_batch* b) { return b ? b->used_bytes : -1; }
+
+int pf_batch_count(const pf_batch* b)
+{
+    if (!b) return -1;
+    int n = 0;
+    for (const auto& s : b->slots) n += s.used ? 1 : 0;
+    return n;
+}
+
+int pf_batch_add(pf_batch* b, const pf_grid* g, const pf_params* p, int* slot)
+{
+    if (!b || !slot) return berr(b, PF_E_ARG, "pf_batch_add: bad argument");
+    *slot = -1;
+    std::string why;
+    int rc = validate(g, p, b->prec, why);
+    if (rc) return berr(b, rc, "pf_batch_add: " + why);
+    if (p->n_varreduras > 2) return berr(b, PF_E_ARG, "pf_batch_add: batches support 1 or 2 sweeps per step");
+    if (b->nsw != 0 && p->n_varreduras != b->nsw && pf_batch_count(b) > 0)
+        return berr(b, PF_E_ARG, "pf_batch_add: every domain of a batch must use the same n_varreduras");
+    int s = -1;
+    for (int i = 0; i < (int)b->slots.size(); ++i)
+        if (!b->slots[i].used) { s = i; break; }
+    if (s < 0) return berr(b, PF_E_NOMEM, "pf_batch_add: all slots are in use");
+    const int px = pitch_of(g->nx);
+    const size_t fb = round_up((size_t)px * g->ny * g->nz * b->es + 64, 256);
+    const size_t bytes = 7 * fb;
+    if (b->budget > 0 && b->used_bytes + (long long)bytes > b->budget)
+        return berr(b, PF_E_NOMEM, "pf_batch_add: over the device-memory budget");
+    Slot& sl = b->slots[s];
+    sl = Slot();
+    void* mem = nullptr;
+    cudaError_t e = cudaMalloc(&mem, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return berr(b, PF_E_NOMEM, std::string("pf_batch_add: cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    cudaMemsetAsync(mem, 0, bytes, b->stream);
+    sl.used = true;
+    sl.g = *g;
+    sl.p = *p;
+    setup_derived(*g, *p, sl.dv);
+    sl.st.it = 0;
+    sl.st.TP = initial_tp(*p);
+    sl.st.M0 = p->M0;
+    sl.st.time = 0.0f;
+    equilibrium(*p, sl.st.TP, &sl.st.Cs_eq, &sl.st.Cl_eq);
+    sl.mem = mem;
+    sl.bytes = bytes;
+    fill_desc(*g, *p, sl.dv, px, sl.bd.d);
+    char* m = (char*)mem;
+    sl.bd.phi[0] = m;
+    sl.bd.phi[1] = m + fb;
+    sl.bd.c[0] = m + 2 * fb;
+    sl.bd.c[1] = m + 3 * fb;
+    sl.bd.T[0] = m + 4 * fb;
+    sl.bd.T[1] = m + 5 * fb;
+    sl.bd.dpp = m + 6 * fb;
+    BCK(cudaMemcpyAsync(b->d_doms + s, &sl.bd, sizeof(BatchDomain), cudaMemcpyHostToDevice, b->stream), "descriptor");
+    BCK(cudaStreamSynchronize(b->stream), "descriptor sync");
+    b->used_bytes += (long long)bytes;
+    b->nsw = p->n_varreduras;
+    b->items_dirty = true;
+    *slot = s;
+    return PF_OK;
+}
+
+int pf_batch_remove(pf_batch* b, int slot)
+{
+    if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used)
+        return berr(b, PF_E_ARG, "pf_batch_remove: bad slot");
+    BCK(cudaStreamSynchronize(b->stream), "remove sync");
+    Slot& sl = b->slots[slot];
+    cudaFree(sl.mem);
+    b->used_bytes -= (long long)sl.bytes;
+    sl = Slot();
+    b->items_dirty = true;
+    return PF_OK;
+}
+
+static void* slot_field(Slot& sl, int field)
+{
+    switch (field) {
+    case PF_PHASE_OLD: return sl.bd.phi[sl.qphi];
+    case PF_PHASE_NEW: return sl.bd.phi[1 - sl.qphi];
+    case PF_CONC_OLD: return sl.bd.c[sl.qc];
+    case PF_CONC_NEW: return sl.bd.c[1 - sl.qc];
+    case PF_TOLD: return sl.bd.T[sl.qT];
+    case PF_TNEW: return sl.bd.T[1 - sl.qT];
+    case PF_DPP: return sl.bd.dpp;
+    }
+    return nullptr;
+}
+
+static Slot* get_slot(pf_batch* b, int slot)
+{
+    if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used) return nullptr;
+    return &b->slots[slot];
+}
+
+int pf_batch_upload(pf_batch* b, int slot, int field, const double* host)
+{
+    Slot* sl = get_slot(b, slot);
+    if (!sl || !host || field < 0 || field > 6) return berr(b, PF_E_ARG, "pf_batch_upload: bad argument");
+    const pf_grid& g = sl->g;
+    void* dst = slot_field(*sl, field);
+    if (b64(b)) {
+        BCK(cudaMemcpy2DAsync(dst, (size_t)sl->bd.d.px * 8, host, (size_t)g.nx * 8, (size_t)g.nx * 8,
+                              (size_t)g.ny * g.nz, cudaMemcpyHostToDevice, b->stream),
+            "pf_batch_upload");
+    } else {
+        // through the staging area of the diagnostics buffer is too small; use a temporary
+        const size_t n = (size_t)g.nx * g.ny * g.nz;
+        double* stage = nullptr;
+        BCK(cudaMalloc(&stage, n * sizeof(double)), "pf_batch_upload staging");
+        cudaError_t e = cudaMemcpyAsync(stage, host, n * sizeof(double), cudaMemcpyHostToDevice, b->stream);
+        if (e == cudaSuccess) e = launch_convert_in<float>(sl->bd.d, stage, dst, 0, g.nz, b->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+        cudaFree(stage);
+        if (e != cudaSuccess) return berr(b, PF_E_CUDA, std::string("pf_batch_upload: ") + cudaGetErrorString(e));
+    }
+    BCK(cudaStreamSynchronize(b->stream), "pf_batch_upload sync");
+    return PF_OK;
+}
+
+int pf_batch_download(pf_batch* b, int slot, int field, double* host)
+{
+    Slot* sl = get_slot(b, slot);
+    if (!sl || !host || field < 0 || field > 6) return berr(b, PF_E_ARG, "pf_batch_download: bad argument");
+    const pf_grid& g = sl->g;
+    void* src = slot_field(*sl, field);
+    if (b64(b)) {
+        BCK(cudaMemcpy2DAsync(host, (size_t)g.nx * 8, src, (size_t)sl->bd.d.px * 8, (size_t)g.nx * 8,
+                              (size_t)g.ny * g.nz, cudaMemcpyDeviceToHost, b->stream),
+            "pf_batch_download");
+    } else {
+        const size_t n = (size_t)g.nx * g.ny * g.nz;
+        double* stage = nullptr;
+        BCK(cudaMalloc(&stage, n * sizeof(double)), "pf_batch_download staging");
+        cudaError_t e = launch_convert_out<float>(sl->bd.d, src, stage, 0, g.nz, b->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(host, stage, n * sizeof(double), cudaMemcpyDeviceToHost, b->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+        cudaFree(stage);
+        if (e != cudaSuccess) return berr(b, PF_E_CUDA, std::string("pf_batch_download: ") + cudaGetErrorString(e));
+    }
+    BCK(cudaStreamSynchronize(b->stream), "pf_batch_download sync");
+    return PF_OK;
+}
+
+int pf_batch_init_seeded(pf_batch* b, int slot, int n_bumps, const double* sites)
+{
+    Slot* sl = get_slot(b, slot);
+    if (!sl || n_bumps < 0 || n_bumps > 4096 || (n_bumps > 0 && !sites))
+        return berr(b, PF_E_ARG, "pf_batch_init_seeded: bad argument (at most 4096 bumps)");
+    InitArgs a;
+    a.n_bumps = n_bumps;
+    a.slab_top = 4.5;
+    a.bump_r = 3.0;
+    a.width = sl->p.Thin_Interface;
+    a.kmax = std::min(sl->g.nz, (int)(a.slab_top + a.bump_r + 20.0 * a.width / 2.0) + 2);
+    a.C0 = sl->p.C0;
+    a.Ke = (double)sl->p.Ke;
+    a.T0 = sl->p.T0;
+    if (n_bumps)
+        BCK(cudaMemcpyAsync(b->d_sites, sites, 2 * n_bumps * sizeof(double), cudaMemcpyHostToDevice, b->stream),
+            "bump sites");
+    cudaError_t e = b64(b) ? launch_init_seeded<double>(sl->bd.d, a, b->d_sites, slot_field(*sl, PF_PHASE_OLD),
+                                                        slot_field(*sl, PF_CONC_OLD), slot_field(*sl, PF_TOLD),
+                                                        sl->bd.dpp, b->stream)
+                           : launch_init_seeded<float>(sl->bd.d, a, b->d_sites, slot_field(*sl, PF_PHASE_OLD),
+                                                       slot_field(*sl, PF_CONC_OLD), slot_field(*sl, PF_TOLD),
+                                                       sl->bd.dpp, b->stream);
+    BCK(e, "pf_batch_init_seeded");
+    BCK(cudaStreamSynchronize(b->stream), "pf_batch_init_seeded sync");
+    return PF_OK;
+}
+
+int pf_batch_set_target(pf_batch* b, int slot, long long target_it)
+{
+    Slot* sl = get_slot(b, slot);
+    if (!sl || target_it < 0) return berr(b, PF_E_ARG, "pf_batch_set_target: bad argument");
+    sl->target = target_it;
+    return PF_OK;
+}
+
+int pf_batch_get_state(const pf_batch* b, int slot, pf_state* out)
+{
+    if (!b || !out || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used) return PF_E_ARG;
+    *out = b->slots[slot].st;
+    return PF_OK;
+}
+
+int pf_batch_set_tile(pf_batch* b, int tile_y, int zchunk)
+{
+    if (!b || (tile_y != 4 && tile_y != 8 && tile_y != 16) || zchunk < 1)
+        return berr(b, PF_E_ARG, "pf_batch_set_tile: tile_y in {4, 8, 16}, zchunk >= 1");
+    if (tile_y != b->tile_y || zchunk != b->zchunk) {
+        b->tile_y = tile_y;
+        b->zchunk = zchunk;
+        b->items_dirty = true;
+        set_grid(b);
+    }
+    return PF_OK;
+}
+
+int pf_batch_step(pf_batch* b, int n_steps)
+{
+    if (!b || n_steps < 0) return berr(b, PF_E_ARG, "pf_batch_step: bad argument");
+    if (b->items_dirty) {
+        int rc = rebuild_items(b);
+        if (rc) return rc;
+    }
+    int rc = capture_graph(b);
+    if (rc) return rc;
+    double ms_total = 0.0;
+    long long steps_done = 0;
+    int left = n_steps;
+    while (left > 0) {
+        const int chunk = std::min(left, kGraphSteps);
+        const int hb = b->h_cur;
+        BCK(cudaEventSynchronize(b->h_ev[hb]), "step table reuse");
+        const int adv = fill_steps(b, b->h_steps[hb], chunk);
+        left -= chunk;
+        if (adv == 0) break;   // every slot reached its target
+        BCK(cudaMemcpyAsync(b->d_steps, b->h_steps[hb], sizeof(BatchStep) * (size_t)kGraphSteps * b->max_domains,
+                            cudaMemcpyHostToDevice, b->stream),
+            "step table upload");
+        BCK(cudaEventRecord(b->h_ev[hb], b->stream), "step table event");
+        b->h_cur ^= 1;
+        BCK(cudaEventRecord(b->ev0, b->stream), "timing event");
+        BCK(cudaGraphLaunch(b->graph, b->stream), "graph launch");
+        BCK(cudaEventRecord(b->ev1, b->stream), "timing event");
+        BCK(cudaEventSynchronize(b->ev1), "graph sync");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+        ms_total += ms;
+        steps_done += adv;
+    }
+    b->last_ms = ms_total;
+    b->last_steps = steps_done;
+    return PF_OK;
+}
+
+double pf_batch_last_ms(const pf_batch* b) { return b ? b->last_ms : -1.0; }
+
+int pf_batch_autotune(pf_batch* b, int steps_per_candidate, int* tile_y, int* zchunk, double* ms_per_step)
+{
+    if (!b || steps_per_candidate < 1) return berr(b, PF_E_ARG, "pf_batch_autotune: bad argument");
+    // shape class: precision, median column count bucket, median depth bucket
+    std::vector<long long> cols, depth;
+    for (const auto& s : b->slots)
+        if (s.used) {
+            cols.push_back((long long)s.g.nx * s.g.ny);
+            depth.push_back(s.g.nz);
+        }
+    if (cols.empty()) return berr(b, PF_E_STATE, "pf_batch_autotune: empty batch");
+    std::nth_element(cols.begin(), cols.begin() + cols.size() / 2, cols.end());
+    std::nth_element(depth.begin(), depth.begin() + depth.size() / 2, depth.end());
+    const auto key = std::make_tuple(b->prec, (int)std::log2((double)cols[cols.size() / 2] + 1),
+                                     (int)std::log2((double)depth[depth.size() / 2] + 1));
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            int rc = pf_batch_set_tile(b, it->second.first, it->second.second);
+            if (tile_y) *tile_y = it->second.first;
+            if (zchunk) *zchunk = it->second.second;
+            if (ms_per_step) *ms_per_step = -1.0;
+            return rc;
+        }
+    }
+    // every candidate runs real steps (results do not depend on the tile
+    // shape), one untimed step first
+    double best = 1e300;
+    int bty = b->tile_y, bzc = b->zchunk;
+    for (int ty : {4, 8, 16})
+        for (int zc : {16, 32, 64, 128}) {
+            int rc = pf_batch_set_tile(b, ty, zc);
+            if (!rc) rc = pf_batch_step(b, 1);
+            if (!rc) rc = pf_batch_step(b, steps_per_candidate);
+            if (rc) return rc;
+            if (b->last_steps == 0) break;
+            const double ms = b->last_ms / (double)b->last_steps;
+            if (ms < best) {
+                best = ms;
+                bty = ty;
+                bzc = zc;
+            }
+        }
+    int rc = pf_batch_set_tile(b, bty, bzc);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[key] = {bty, bzc};
+    }
+    if (tile_y) *tile_y = bty;
+    if (zchunk) *zchunk = bzc;
+    if (ms_per_step) *ms_per_step = best;
+    return rc;
+}
+
+int pf_batch_diagnosticos(pf_batch* b, int slot, double out[5])
+{
+    Slot* sl = get_slot(b, slot);
+    if (!sl || !out) return berr(b, PF_E_ARG, "pf_batch_diagnosticos: bad argument");
+    double* res = b->d_part + 592 * 8;
+    cudaError_t e = b64(b) ? launch_diag<double>(sl->bd.d, slot_field(*sl, PF_PHASE_OLD), slot_field(*sl, PF_CONC_OLD),
+                                                 b->d_part, 592, res, b->stream)
+                           : launch_diag<float>(sl->bd.d, slot_field(*sl, PF_PHASE_OLD), slot_field(*sl, PF_CONC_OLD),
+                                                b->d_part, 592, res, b->stream);
+    BCK(e, "pf_batch_diagnosticos");
+    BCK(cudaMemcpyAsync(b->h_out, res, 5 * sizeof(double), cudaMemcpyDeviceToHost, b->stream), "diag copy");
+    BCK(cudaStreamSynchronize(b->stream), "diag sync");
+    std::memcpy(out, b->h_out, 5 * sizeof(double));
+    return PF_OK;
+}
+
+}  // extern "C"

@@ -100,6 +100,26 @@ __device__ __forceinline__ double ruido_suave64(int i, int j, int k, int it)
     return __dadd_rn(__dmul_rn(1.0 - fz, lo), __dmul_rn(fz, hi));
 }
 
+// The hash input of variaveis.f90:82-83 without the k term; adding k*C for
+// each plane gives the input of cell (i, j, k) (wrapping 64-bit arithmetic).
+__host__ __device__ __forceinline__ uint64_t hash_base(int i, int j, int it, int salt)
+{
+    return (uint64_t)(int64_t)i * 2654435761ull + (uint64_t)(int64_t)j * 2246822519ull +
+           (uint64_t)(int64_t)it * 668265263ull + (uint64_t)(int64_t)salt * 374761393ull + 1ull;
+}
+constexpr uint64_t kHashK = 3266489917ull;
+
+// fmix64 rounds of variaveis.f90:84-88 on a precomputed input
+__host__ __device__ __forceinline__ uint64_t hash63_mix(uint64_t h)
+{
+    h ^= h >> 33;
+    h *= 0xff51afd7ed558ccdull;
+    h ^= h >> 33;
+    h *= 0xc4ceb9fe1a85ec53ull;
+    h ^= h >> 33;
+    return h & 0x7fffffffffffffffull;
+}
+
 // The REAL(4) `ran` of phase_body.inc:181-185 (identical for both precisions).
 __device__ __forceinline__ float phase_ran(int rt, int i, int j, int k, int it)
 {
@@ -121,6 +141,13 @@ template <> struct Ar<float> {
     static __device__ __forceinline__ float lg(float x) { return logf(x); }
     static __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
 };
+
+// Explicit multiply-add.  Every translation unit is built without automatic
+// contraction, so the same source gives the same bits in every kernel that
+// inlines it (single domain, batch, any tile shape); the fast form asks for
+// its multiply-adds here.
+__device__ __forceinline__ double fmadd(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fmadd(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 
 // Loop-invariant constants converted to the stencil type once per block.
 template <typename T>
@@ -179,23 +206,49 @@ __device__ __forceinline__ Node<T> aniso_node(T gx, T gy, T gz, const KC<T>& c)
 {
     Node<T> n;
     T gx2 = gx * gx, gy2 = gy * gy, gz2 = gz * gz;
-    T Q = gx2 + gy2 + gz2 + (T)1e-23;
-    T S4 = gx2 * gx2 + gy2 * gy2 + gz2 * gz2;
-    T Q2 = Q * Q;
     if constexpr (!FAST) {
+        T Q = gx2 + gy2 + gz2 + (T)1e-23;
+        T S4 = gx2 * gx2 + gy2 * gy2 + gz2 * gz2;
+        T Q2 = Q * Q;
         n.eps = c.E0 * ((T)1 + c.DE * ((T)4 * S4 / Q2 - (T)3));
         T Ke_ = c.K * n.eps;
         n.exy = Ke_ * gx * gy * (gx2 - gy2) / Q2;
         n.eyz = Ke_ * gy * gz * (gy2 - gz2) / Q2;
         n.ezx = Ke_ * gz * gx * (gz2 - gx2) / Q2;
-    } else {
-        T rq = Ar<T>::rcp(Q2);
-        n.eps = c.E0 * ((T)1 + c.DE * ((T)4 * S4 * rq - (T)3));
+    } else if constexpr (sizeof(T) == 8) {
+        T Q = fmadd(gx, gx, fmadd(gy, gy, fmadd(gz, gz, (T)1e-23)));
+        T S4 = fmadd(gx2, gx2, fmadd(gy2, gy2, gz2 * gz2));
+        T rq = Ar<T>::rcp(Q * Q);
+        n.eps = c.E0 * fmadd(c.DE, fmadd((T)4 * S4, rq, (T)-3), (T)1);
         T f = c.K * n.eps * rq;
         n.exy = f * gx * gy * (gx2 - gy2);
         n.eyz = f * gy * gz * (gy2 - gz2);
         n.ezx = f * gz * gx * (gz2 - gx2);
+    } else {
+        // FP32: Q^2 >= 1e-46 is below the FP32 range, so evaluate the
+        // scale-invariant form with g normalised by its largest component m:
+        // 4 S4/Q^2 and e_ab are unchanged, and `small` becomes 1e-23/m^2.
+        // For m < 1e-15 the reference's ratio and cross terms are below
+        // 1e-13 relative (Q is dominated by small): the flat-node values.
+        const T m = fmaxf(fabsf(gx), fmaxf(fabsf(gy), fabsf(gz)));
+        if (m < (T)1e-15) {
+            n.eps = c.E0 * fmadd(c.DE, (T)-3, (T)1);
+            n.exy = n.eyz = n.ezx = (T)0;
+        } else {
+            const T im = Ar<T>::rcp(m);
+            const T ux = gx * im, uy = gy * im, uz = gz * im;
+            const T ux2 = ux * ux, uy2 = uy * uy, uz2 = uz * uz;
+            const T Q = fmadd(ux, ux, fmadd(uy, uy, fmadd(uz, uz, (T)1e-23 * im * im)));
+            const T S4 = fmadd(ux2, ux2, fmadd(uy2, uy2, uz2 * uz2));
+            const T rq = Ar<T>::rcp(Q * Q);
+            n.eps = c.E0 * fmadd(c.DE, fmadd((T)4 * S4, rq, (T)-3), (T)1);
+            const T f = c.K * n.eps * rq;
+            n.exy = f * ux * uy * (ux2 - uy2);
+            n.eyz = f * uy * uz * (uy2 - uz2);
+            n.ezx = f * uz * ux * (uz2 - ux2);
+        }
     }
+    (void)gx2; (void)gy2; (void)gz2;
     return n;
 }
 
@@ -253,17 +306,21 @@ __device__ __forceinline__ T phase_ppnew(const Nbr<T>& p, const Node<T>& E, cons
             ruidos = (two * (T)ran - one) * c.AAA * (T)16 * pp2 * (q * q);
         return PP + c.M0dt * (AA + GG) + ruidos;
     } else {
-        T AA = (E.eps * E.eps * (p.PE - PP) + W.eps * W.eps * (p.PW - PP)) * c.rdx2 +
-               (N.eps * N.eps * (p.PN - PP) + S.eps * S.eps * (p.PS - PP)) * c.rdy2 +
-               (Tt.eps * Tt.eps * (p.PT - PP) + B.eps * B.eps * (p.PB - PP)) * c.rdz2;
+        T ax = fmadd(E.eps * E.eps, p.PE - PP, W.eps * W.eps * (p.PW - PP));
+        T ay = fmadd(N.eps * N.eps, p.PN - PP, S.eps * S.eps * (p.PS - PP));
+        T az = fmadd(Tt.eps * Tt.eps, p.PT - PP, B.eps * B.eps * (p.PB - PP));
+        T AA = fmadd(ax, c.rdx2, fmadd(ay, c.rdy2, az * c.rdz2));
         // cross terms of phase_body.inc:137-147 grouped by node
-        T Cxy = E.exy * (p.PNE - p.PSE + p.PN - p.PS) + N.exy * (p.PNW - p.PNE + p.PW - p.PE) +
-                W.exy * (p.PSW - p.PNW + p.PS - p.PN) + S.exy * (p.PSE - p.PSW + p.PE - p.PW);
-        T Cyz = N.eyz * (p.PNT - p.PNB + p.PT - p.PB) + Tt.eyz * (p.PST - p.PNT + p.PS - p.PN) +
-                S.eyz * (p.PSB - p.PST + p.PB - p.PT) + B.eyz * (p.PNB - p.PSB + p.PN - p.PS);
-        T Czx = Tt.ezx * (p.PET - p.PWT + p.PE - p.PW) + W.ezx * (p.PWT - p.PWB + p.PT - p.PB) +
-                B.ezx * (p.PWB - p.PEB + p.PW - p.PE) + E.ezx * (p.PEB - p.PET + p.PB - p.PT);
-        AA = AA + c.cxy * Cxy + c.cyz * Cyz + c.czx * Czx;
+        T Cxy = fmadd(E.exy, (p.PNE - p.PSE) + (p.PN - p.PS),
+                      fmadd(N.exy, (p.PNW - p.PNE) + (p.PW - p.PE),
+                            fmadd(W.exy, (p.PSW - p.PNW) + (p.PS - p.PN), S.exy * ((p.PSE - p.PSW) + (p.PE - p.PW)))));
+        T Cyz = fmadd(N.eyz, (p.PNT - p.PNB) + (p.PT - p.PB),
+                      fmadd(Tt.eyz, (p.PST - p.PNT) + (p.PS - p.PN),
+                            fmadd(S.eyz, (p.PSB - p.PST) + (p.PB - p.PT), B.eyz * ((p.PNB - p.PSB) + (p.PN - p.PS)))));
+        T Czx = fmadd(Tt.ezx, (p.PET - p.PWT) + (p.PE - p.PW),
+                      fmadd(W.ezx, (p.PWT - p.PWB) + (p.PT - p.PB),
+                            fmadd(B.ezx, (p.PWB - p.PEB) + (p.PW - p.PE), E.ezx * ((p.PEB - p.PET) + (p.PB - p.PT)))));
+        AA = fmadd(c.cxy, Cxy, fmadd(c.cyz, Cyz, fmadd(c.czx, Czx, AA)));
         const T q = one - PP;
         T g_linha = two * PP * q * (one - two * PP);
         T h_linha, h;
@@ -274,13 +331,13 @@ __device__ __forceinline__ T phase_ppnew(const Nbr<T>& p, const Node<T>& E, cons
             h_linha = (T)6 * PP * q;
             h = PP * PP * ((T)3 - two * PP);
         }
-        T den = one - c.omKe * h;
+        T den = fmadd(-c.omKe, h, one);
         // (1-CLP)/(1-CSP) = (den - c)/(den - Ke c); the constant factor is in Lc
-        T lg = Ar<T>::lg(fabs(Ar<T>::div(den - CPP, den - c.Ke * CPP))) + c.Lc;
-        T GG = c.RTV * h_linha * lg - c.W0 * g_linha;
+        T lg = Ar<T>::lg(fabs(Ar<T>::div(den - CPP, fmadd(-c.Ke, CPP, den)))) + c.Lc;
+        T GG = fmadd(c.RTV * h_linha, lg, -(c.W0 * g_linha));
         T pp2q2 = PP * PP * q * q * c.AAA16;
-        T ruidos = (c.rt == 0) ? (T)ran * pp2q2 : (two * (T)ran - one) * pp2q2;
-        return PP + c.M0dt * (AA + GG) + ruidos;
+        T ruidos = (c.rt == 0) ? (T)ran * pp2q2 : fmadd(two, (T)ran, -one) * pp2q2;
+        return fmadd(c.M0dt, AA + GG, PP + ruidos);
     }
 }
 
@@ -319,10 +376,10 @@ __device__ __forceinline__ SolNode<T> sol_node(T P, T C, const KC<T>& c)
         n.br = (one - h) * CL * (one - CL) + h * CS * (one - CS);
         n.mu = log(CL / (one - CL));
     } else {
-        T den = one - c.omKe * h;
+        T den = fmadd(-c.omKe, h, one);
         T CL = C * Ar<T>::rcp(den);
         T CS = c.Ke * CL;
-        n.br = (one - h) * CL * (one - CL) + h * CS * (one - CS);
+        n.br = fmadd((one - h) * CL, one - CL, h * CS * (one - CS));
         n.mu = Ar<T>::lg(Ar<T>::div(C, den - C));   // CL/(1-CL) = C/(den-C)
     }
     return n;
@@ -357,10 +414,10 @@ __device__ __forceinline__ T conc_new(T PP, T CPP, const SolNode<T>& P, const So
             T sum = P.br + b;
             return (sum > (T)0) ? D2 * b * Ar<T>::rcp(sum) : (T)0;
         };
-        T fx = hm(E.br) * (E.mu - P.mu) - hm(W.br) * (P.mu - W.mu);
-        T fy = hm(N.br) * (N.mu - P.mu) - hm(S.br) * (P.mu - S.mu);
-        T fz = hm(Tt.br) * (Tt.mu - P.mu) - hm(B.br) * (P.mu - B.mu);
-        return CPP + (c.dtIX * fx + c.dtIY * fy + c.dtIZ * fz);
+        T fx = fmadd(hm(E.br), E.mu - P.mu, -(hm(W.br) * (P.mu - W.mu)));
+        T fy = fmadd(hm(N.br), N.mu - P.mu, -(hm(S.br) * (P.mu - S.mu)));
+        T fz = fmadd(hm(Tt.br), Tt.mu - P.mu, -(hm(B.br) * (P.mu - B.mu)));
+        return CPP + fmadd(c.dtIX, fx, fmadd(c.dtIY, fy, c.dtIZ * fz));
     }
 }
 

@@ -1,6 +1,7 @@
 // pf3d_fp32.cu -- FP32 instantiation of every kernel (fields and stencils in FP32;
-// diagnostics still accumulate in FP64).  Multiply-adds may be contracted.
+// diagnostics still accumulate in FP64).
 #include "pf3d_simple.cuh"
+#include "pf3d_init.cuh"
 #include "pf3d_fused.cuh"
 
 namespace pf3d {
@@ -13,4 +14,12 @@ template cudaError_t launch_fused_last<float>(const DomainDesc&, const StepArgs&
 template cudaError_t launch_diag<float>(const DomainDesc&, const void*, const void*, double*, int, double*, cudaStream_t);
 template cudaError_t launch_convert_in<float>(const DomainDesc&, const double*, void*, long long, long long, cudaStream_t);
 template cudaError_t launch_convert_out<float>(const DomainDesc&, const void*, double*, long long, long long, cudaStream_t);
+template cudaError_t launch_fused_batch<float>(const BatchDomain*, const BatchStep*, const BatchItem*, const int*, int, bool, int, int, int, cudaStream_t);
+template int batch_blocks_per_sm<float>(int);
+template <>
+cudaError_t launch_init_seeded<float>(const DomainDesc& d, const InitArgs& a, const double* sites, void* phi, void* c,
+                                  void* Tf, void* dpp, cudaStream_t st)
+{
+    return launch_init_seeded_impl<float>(d, a, sites, phi, c, Tf, dpp, st);
+}
 }  // namespace pf3d

@@ -62,22 +62,24 @@ struct FusedOcc {
 __device__ __forceinline__ int add5(int a, int k) { int t = a + k; return t >= 5 ? t - 5 : t; }
 __device__ __forceinline__ int add3(int a, int k) { int t = a + k; return t >= 3 ? t - 3 : t; }
 
+// One 32 x TY x zchunk tile (tile coordinates bx, by, bz) of one domain.
+// Ends with a CTA-wide barrier, so the caller may reuse the shared memory.
 template <typename T, int TY, bool HEAT, bool DPPW, bool SOL>
-__global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY>::v))
-    k_fused(DomainDesc d, StepArgs s, const T* __restrict__ phi_in, const T* __restrict__ c_in,
-            T* __restrict__ phi_out, T* __restrict__ dpp, T* __restrict__ c_out, const T* __restrict__ T_old,
-            T* __restrict__ T_new, int zchunk)
+__device__ __forceinline__ void fused_tile(const DomainDesc& d, const StepArgs& s, const T* __restrict__ phi_in,
+                                           const T* __restrict__ c_in, T* __restrict__ phi_out,
+                                           T* __restrict__ dpp, T* __restrict__ c_out,
+                                           const T* __restrict__ T_old, T* __restrict__ T_new, int zchunk, int bx,
+                                           int by, int bz, unsigned char* smem_raw)
 {
     using SM = FusedSmem<T, TY>;
     constexpr int TX = SM::TX, PW = SM::PW, PH = SM::PH, NW = SM::NW, NH = SM::NH;
     constexpr int RING = 2 * NW + 2 * TY;   // ring nodes around the tile
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     SM& sm = *reinterpret_cast<SM*>(smem_raw);
 
     const int nx = d.nx, ny = d.ny, nz = d.nz;
     const long long px = d.px, pl = d.plane;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-    const int zb = blockIdx.z * zchunk;
+    const int x0 = bx * TX, y0 = by * TY;
+    const int zb = bz * zchunk;
     const int ze = min(zb + zchunk, nz);
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int tid = tx + TX * ty;
@@ -200,8 +202,10 @@ __global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY>::v))
     if (own && xs_src) fpre_range(x, nx, &xl, &xh);
     if (own && ys_src) fpre_range(y, ny, &yl, &yh);
     long long zoff = (long long)zb * pl;
+    // noise hash input of the own cell, carried along z (k = z + 1)
+    uint64_t hin = hash_base(x + 1, y + 1, c.it, 1) + (uint64_t)(zb + 1) * kHashK;
 
-    for (int z = zb; z < ze; ++z, zoff += pl) {
+    for (int z = zb; z < ze; ++z, zoff += pl, hin += kHashK) {
         const long long id = col + zoff;
         // centre values from global memory, consumed after the node pass
         T cpp = 0, dppv = 0, told = 0;
@@ -264,7 +268,8 @@ __global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY>::v))
                     Tt.eps = sm.eps[np1][nly][nlx]; Tt.eyz = sm.eyz[np1][nly][nlx]; Tt.ezx = sm.ezx[np1][nly][nlx];
                     B.eps = sm.eps[nm1][nly][nlx]; B.eyz = sm.eyz[nm1][nly][nlx]; B.ezx = sm.ezx[nm1][nly][nlx];
                     E.eyz = W.eyz = N.ezx = S.ezx = Tt.exy = B.exy = (T)0;   // unused by the body
-                    float ran = phase_ran(c.rt, x + 1, y + 1, z + 1, c.it);
+                    float ran = (c.rt == 2) ? phase_ran(2, x + 1, y + 1, z + 1, c.it)
+                                            : __double2float_rn(ran64(hash63_mix(hin)));
                     T ppn = phase_ppnew<T, true>(nb, E, W, N, S, Tt, B, cpp, ran, c);
                     if (DPPW) dpp[id] = ppn - PPc;
                     U = clamp01(ppn);
@@ -316,6 +321,52 @@ __global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY>::v))
         __syncthreads();
         s5 = add5(s5, 1);
         s3 = add3(s3, 1);
+    }
+    __syncthreads();
+}
+
+// single domain: one CTA per tile
+template <typename T, int TY, bool HEAT, bool DPPW, bool SOL>
+__global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY>::v))
+    k_fused(DomainDesc d, StepArgs s, const T* __restrict__ phi_in, const T* __restrict__ c_in,
+            T* __restrict__ phi_out, T* __restrict__ dpp, T* __restrict__ c_out, const T* __restrict__ T_old,
+            T* __restrict__ T_new, int zchunk)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    fused_tile<T, TY, HEAT, DPPW, SOL>(d, s, phi_in, c_in, phi_out, dpp, c_out, T_old, T_new, zchunk, blockIdx.x,
+                                       blockIdx.y, blockIdx.z, smem_raw);
+}
+
+// many domains: a persistent grid walks the work list.  PASS 0 is the first
+// pass of a step (temperatura + sweep 1, or the whole step with one sweep),
+// PASS 1 the last (sweep 2 + solute).
+template <typename T, int TY, int PASS, bool ONE_SWEEP>
+__global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY>::v))
+    k_fused_batch(const BatchDomain* __restrict__ doms, const BatchStep* __restrict__ steps,
+                  const BatchItem* __restrict__ items, const int* __restrict__ n_items, int zchunk)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = *n_items;
+    for (int w = blockIdx.x; w < n; w += gridDim.x) {
+        const BatchItem it = items[w];
+        const BatchStep& st = steps[it.dom];
+        if (!st.active) continue;   // uniform across the CTA
+        const BatchDomain& D = doms[it.dom];
+        const int q = st.q_phi, qc = st.q_c, qt = st.q_T;
+        if (PASS == 0) {
+            if (ONE_SWEEP)
+                fused_tile<T, TY, true, true, true>(D.d, st.s, (const T*)D.phi[q], (const T*)D.c[qc], (T*)D.phi[1 - q],
+                                                    (T*)D.dpp, (T*)D.c[1 - qc], (const T*)D.T[qt], (T*)D.T[1 - qt],
+                                                    zchunk, it.bx, it.by, it.bz, smem_raw);
+            else
+                fused_tile<T, TY, true, false, false>(D.d, st.s, (const T*)D.phi[q], (const T*)D.c[qc],
+                                                      (T*)D.phi[1 - q], (T*)D.dpp, nullptr, (const T*)D.T[qt],
+                                                      (T*)D.T[1 - qt], zchunk, it.bx, it.by, it.bz, smem_raw);
+        } else {
+            fused_tile<T, TY, false, true, true>(D.d, st.s, (const T*)D.phi[1 - q], (const T*)D.c[qc], (T*)D.phi[q],
+                                                 (T*)D.dpp, (T*)D.c[1 - qc], nullptr, nullptr, zchunk, it.bx, it.by,
+                                                 it.bz, smem_raw);
+        }
     }
 }
 
@@ -377,6 +428,60 @@ cudaError_t launch_fused_last(const DomainDesc& d, const StepArgs& s, const Fiel
 {
     return launch_fused_ty<T, false, true, true>(d, s, f.phi_mid, f.c_old, f.phi_new, f.dpp, f.c_new, nullptr, nullptr,
                                                  tile_y, zchunk, st);
+}
+
+template <typename T, int TY, int PASS, bool ONE_SWEEP>
+cudaError_t launch_batch_t(const BatchDomain* doms, const BatchStep* steps, const BatchItem* items, const int* n_items,
+                           int zchunk, int grid, cudaStream_t st)
+{
+    auto kern = k_fused_batch<T, TY, PASS, ONE_SWEEP>;
+    const size_t smem = fused_smem_bytes<T, TY>();
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    kern<<<grid, dim3(32, TY), smem, st>>>(doms, steps, items, n_items, zchunk);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_fused_batch(const BatchDomain* doms, const BatchStep* steps, const BatchItem* items,
+                               const int* n_items, int pass, bool one_sweep, int tile_y, int zchunk, int grid,
+                               cudaStream_t st)
+{
+#define PF3D_BATCH_CASE(TYV)                                                                                   \
+    if (tile_y == TYV) {                                                                                       \
+        if (pass == 0)                                                                                         \
+            return one_sweep ? launch_batch_t<T, TYV, 0, true>(doms, steps, items, n_items, zchunk, grid, st)  \
+                             : launch_batch_t<T, TYV, 0, false>(doms, steps, items, n_items, zchunk, grid, st); \
+        return launch_batch_t<T, TYV, 1, false>(doms, steps, items, n_items, zchunk, grid, st);               \
+    }
+    PF3D_BATCH_CASE(4)
+    PF3D_BATCH_CASE(16)
+    PF3D_BATCH_CASE(8)
+#undef PF3D_BATCH_CASE
+    return cudaErrorInvalidValue;
+}
+
+template <typename T>
+int batch_blocks_per_sm(int tile_y)
+{
+    int nb = 0;
+    const void* fn = nullptr;
+    size_t smem = 0;
+    switch (tile_y) {
+    case 4: fn = (const void*)k_fused_batch<T, 4, 1, false>; smem = fused_smem_bytes<T, 4>(); break;
+    case 16: fn = (const void*)k_fused_batch<T, 16, 1, false>; smem = fused_smem_bytes<T, 16>(); break;
+    default: fn = (const void*)k_fused_batch<T, 8, 1, false>; smem = fused_smem_bytes<T, 8>(); break;
+    }
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, 32 * tile_y, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return nb > 0 ? nb : 1;
 }
 
 }  // namespace pf3d

@@ -1,10 +1,11 @@
 // pf3d_fused64.cu -- FP64 instantiation of the fused z-marching passes.
-// The fused passes use the fast form of the per-cell arithmetic, so this unit
-// is built with multiply-add contraction allowed (FP64 throughout; results
-// within 1e-12 of the reference form).
+// The fused passes use the fast form of the per-cell arithmetic (explicit
+// multiply-adds; FP64 throughout; results within 1e-12 of the reference form).
 #include "pf3d_fused.cuh"
 
 namespace pf3d {
 template cudaError_t launch_fused_first<double>(const DomainDesc&, const StepArgs&, const Fields&, bool, int, int, cudaStream_t);
 template cudaError_t launch_fused_last<double>(const DomainDesc&, const StepArgs&, const Fields&, int, int, cudaStream_t);
+template cudaError_t launch_fused_batch<double>(const BatchDomain*, const BatchStep*, const BatchItem*, const int*, int, bool, int, int, int, cudaStream_t);
+template int batch_blocks_per_sm<double>(int);
 }  // namespace pf3d

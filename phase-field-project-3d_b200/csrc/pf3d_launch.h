@@ -36,6 +36,30 @@ template <typename T> cudaError_t launch_fused_first(const DomainDesc& d, const 
 template <typename T> cudaError_t launch_fused_last(const DomainDesc& d, const StepArgs& s, const Fields& f,
                                                     int tile_y, int zchunk, cudaStream_t st);
 
+// ---- batches of independent domains (persistent work-list kernels) ----
+struct BatchDomain {
+    DomainDesc d;
+    void* phi[2];    // phase field buffers
+    void* c[2];      // solute buffers
+    void* T[2];      // temperature buffers
+    void* dpp;
+};
+// per domain and step: the step scalars, whether the domain advances in this
+// step, and which buffer of each pair holds the "old" field
+struct BatchStep {
+    StepArgs s;
+    int active;
+    int q_phi, q_c, q_T;
+};
+struct BatchItem {
+    int dom, bx, by, bz;
+};
+template <typename T> cudaError_t launch_fused_batch(const BatchDomain* doms, const BatchStep* steps,
+                                                     const BatchItem* items, const int* n_items, int pass,
+                                                     bool one_sweep, int tile_y, int zchunk, int grid,
+                                                     cudaStream_t st);
+template <typename T> int batch_blocks_per_sm(int tile_y);
+
 // Diagnostics: block partials into part[nblk*8], final into out[5].
 template <typename T> cudaError_t launch_diag(const DomainDesc& d, const void* phi, const void* c, double* part,
                                               int nblk, double* out, cudaStream_t st);

@@ -205,3 +205,116 @@ class Domain:
         """Current state after a step: the old fields + DPP (host copies)."""
         return {"phi": self.download(PF_PHASE_OLD), "c": self.download(PF_CONC_OLD),
                 "T": self.download(PF_TOLD), "dpp": self.download(PF_DPP)}
+
+
+def _sites_ptr(sites):
+    a = np.ascontiguousarray(np.asarray(sites, dtype=np.float64).reshape(-1))
+    return a, a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def init_seeded(dom: "Domain", sites) -> None:
+    """Device-side seeded initial state of a Domain (pf_init_seeded)."""
+    a, ptr = _sites_ptr(sites)
+    dom._chk(LIB.pf_init_seeded(dom.handle, len(a) // 2, ptr))
+
+
+class Batch:
+    """Many independent domains stepped together (pf_batch_*)."""
+
+    def __init__(self, precision: int = PF_FP32, budget_bytes: int = 0, max_domains: int = 4096):
+        h = C.c_void_p()
+        check(LIB.pf_batch_create(precision, int(budget_bytes), int(max_domains), C.byref(h)))
+        self._h = h
+        self.precision = precision
+        self.grids = {}
+
+    def close(self):
+        if self._h:
+            LIB.pf_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _chk(self, rc):
+        check(rc, None)
+
+    def set_stream(self, stream_handle):
+        self._chk(LIB.pf_batch_set_stream(self._h, C.c_void_p(stream_handle) if stream_handle else None))
+
+    def add(self, g: pf_grid, p: pf_params) -> int:
+        s = C.c_int()
+        self._chk(LIB.pf_batch_add(self._h, C.byref(g), C.byref(p), C.byref(s)))
+        self.grids[s.value] = g
+        return s.value
+
+    def remove(self, slot: int):
+        self._chk(LIB.pf_batch_remove(self._h, slot))
+        self.grids.pop(slot, None)
+
+    def count(self) -> int:
+        return LIB.pf_batch_count(self._h)
+
+    def bytes_used(self) -> int:
+        return LIB.pf_batch_bytes_used(self._h)
+
+    def upload(self, slot: int, field, host: np.ndarray):
+        q = FIELDS[field] if isinstance(field, str) else int(field)
+        a = np.ascontiguousarray(host, dtype=np.float64)
+        self._chk(LIB.pf_batch_upload(self._h, slot, q, _dptr(a)))
+
+    def download(self, slot: int, field) -> np.ndarray:
+        q = FIELDS[field] if isinstance(field, str) else int(field)
+        g = self.grids[slot]
+        out = np.empty((g.nz, g.ny, g.nx), dtype=np.float64)
+        self._chk(LIB.pf_batch_download(self._h, slot, q, _dptr(out)))
+        return out
+
+    def load_state(self, slot: int, st: dict):
+        self.upload(slot, PF_PHASE_OLD, st["phi"])
+        self.upload(slot, PF_CONC_OLD, st["c"])
+        self.upload(slot, PF_TOLD, st["T"])
+        self.upload(slot, PF_DPP, st.get("dpp", np.zeros_like(st["phi"])))
+
+    def init_seeded(self, slot: int, sites):
+        a, ptr = _sites_ptr(sites)
+        self._chk(LIB.pf_batch_init_seeded(self._h, slot, len(a) // 2, ptr))
+
+    def set_target(self, slot: int, target_it: int):
+        self._chk(LIB.pf_batch_set_target(self._h, slot, int(target_it)))
+
+    def state(self, slot: int) -> pf_state:
+        st = pf_state()
+        self._chk(LIB.pf_batch_get_state(self._h, slot, C.byref(st)))
+        return st
+
+    def step(self, n: int = 1) -> float:
+        """Advance every active slot by up to n steps; returns device ms."""
+        self._chk(LIB.pf_batch_step(self._h, int(n)))
+        return LIB.pf_batch_last_ms(self._h)
+
+    def set_tile(self, tile_y: int, zchunk: int):
+        self._chk(LIB.pf_batch_set_tile(self._h, tile_y, zchunk))
+
+    def autotune(self, steps_per_candidate: int = 2):
+        ty, zc, ms = C.c_int(), C.c_int(), C.c_double()
+        self._chk(LIB.pf_batch_autotune(self._h, steps_per_candidate, C.byref(ty), C.byref(zc), C.byref(ms)))
+        return ty.value, zc.value, ms.value
+
+    def diagnosticos(self, slot: int):
+        out = (C.c_double * 5)()
+        self._chk(LIB.pf_batch_diagnosticos(self._h, slot, out))
+        return tuple(out)
+
+    def fields(self, slot: int) -> dict:
+        return {"phi": self.download(slot, PF_PHASE_OLD), "c": self.download(slot, PF_CONC_OLD),
+                "T": self.download(slot, PF_TOLD), "dpp": self.download(slot, PF_DPP)}

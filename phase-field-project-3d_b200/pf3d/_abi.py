@@ -81,6 +81,24 @@ SIGNATURES = [
     ("pf_swap", C.c_int, [_P]),
     ("pf_step", C.c_int, [_P, C.c_int]),
     ("pf_step_diag", C.c_int, [_P, C.c_int, _D]),
+    ("pf_init_seeded", C.c_int, [_P, C.c_int, _D]),
+    ("pf_batch_create", C.c_int, [C.c_int, C.c_longlong, C.c_int, C.POINTER(_P)]),
+    ("pf_batch_destroy", C.c_int, [_P]),
+    ("pf_batch_set_stream", C.c_int, [_P, _P]),
+    ("pf_batch_bytes_used", C.c_longlong, [_P]),
+    ("pf_batch_count", C.c_int, [_P]),
+    ("pf_batch_add", C.c_int, [_P, C.POINTER(pf_grid), C.POINTER(pf_params), C.POINTER(C.c_int)]),
+    ("pf_batch_remove", C.c_int, [_P, C.c_int]),
+    ("pf_batch_upload", C.c_int, [_P, C.c_int, C.c_int, _P]),
+    ("pf_batch_download", C.c_int, [_P, C.c_int, C.c_int, _P]),
+    ("pf_batch_init_seeded", C.c_int, [_P, C.c_int, C.c_int, _D]),
+    ("pf_batch_set_target", C.c_int, [_P, C.c_int, C.c_longlong]),
+    ("pf_batch_get_state", C.c_int, [_P, C.c_int, C.POINTER(pf_state)]),
+    ("pf_batch_step", C.c_int, [_P, C.c_int]),
+    ("pf_batch_last_ms", C.c_double, [_P]),
+    ("pf_batch_set_tile", C.c_int, [_P, C.c_int, C.c_int]),
+    ("pf_batch_autotune", C.c_int, [_P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _D]),
+    ("pf_batch_diagnosticos", C.c_int, [_P, C.c_int, _D]),
     ("pf_diagnosticos_noalloc", C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                           C.c_double, C.c_double, C.c_double, C.c_double, _P, _D]),
 ]
