@@ -170,6 +170,64 @@ def run_reference(args, rank: int, world: int):
     return 0
 
 
+def bench_fp32(args, torch, pf3d, deck, init, stream, world):
+    """1024^3 FP32 (configuration 3), state created on the device."""
+    w = deck.WORKLOADS["c3_1024cube_fp32"]
+    g, p = w.grid(), w.params()
+    d = pf3d.Domain(g, p, pf3d.PF_FP32)
+    d.set_stream(stream.cuda_stream)
+    pf3d.init_seeded(d, init.bump_sites(w.nx, w.ny, w.n_bumps, w.seed))
+    d.step(args.warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n = max(4, args.steps // 2)
+    e0.record(stream)
+    d.step(n)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / n
+    peak, _ = measured_peaks()
+    v = w.cells * world / (ms / 1e3) / 1e9
+    d.close()
+    return {"workload": w.name, "cells": w.cells, "steps": n, "ms_per_step": ms, "value": v, "unit": UNIT,
+            "hbm_frac_step": v / world * STEP_BYTES_PER_CELL[32] / peak, "init": "device (pf_init_seeded)"}
+
+
+def bench_batch(args, pf3d, serve, init):
+    """96 FP32 domains of uneven size (configuration 4), autotuned tiles."""
+    jobs = serve.batch_domains(seed=3)
+    b = pf3d.Batch(pf3d.PF_FP32)
+    for j in jobs:
+        s = b.add(j.grid(), j.params())
+        b.init_seeded(s, j.sites())
+        j.slot = s
+    t0 = time.perf_counter()
+    ty, zc, _ = b.autotune(2)
+    tune_s = time.perf_counter() - t0
+    b.step(8)
+    n = max(16, args.steps)
+    ms = b.step(n)
+    cells = sum(j.cells for j in jobs)
+    b.close()
+    return {"workload": "c4_96_domains_fp32", "domains": len(jobs), "cells": cells, "steps": n,
+            "ms_per_step": ms / n, "value": cells * n / (ms / 1e3) / 1e9, "unit": UNIT,
+            "tile": [32, ty, zc], "autotune_s": tune_s, "launch": "persistent work-list kernels, CUDA graph of 8 steps"}
+
+
+def bench_serve(args, serve):
+    """Bounded sample of the serving configuration (5): the first requests of
+    the seeded Poisson stream, every step count scaled by step_scale."""
+    jobs = serve.request_stream(seed=4, n=args.serve_requests, step_scale=args.serve_step_scale)
+    srv = serve.Server(budget_bytes=150e9, quantum=8)
+    try:
+        st = srv.run(jobs)
+    finally:
+        srv.close()
+    st.update({"workload": "c5_poisson_20_per_s_seed4", "sample": f"first {len(jobs)} requests, steps x {args.serve_step_scale}",
+               "fp64_share": sum(1 for j in jobs if j.precision == 64) / len(jobs), "budget_gb": 150})
+    return st
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -180,6 +238,11 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--serve-step-scale", type=float, default=0.05)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -296,6 +359,17 @@ def main():
 
     dom.close()
 
+    extra = {}
+    if not args.no_fp32:
+        extra["fp32"] = bench_fp32(args, torch, pf3d, deck, init, stream, world)
+        extra["fp32"]["speedup_vs_fp64"] = extra["fp32"]["value"] / value
+    if rank == 0 and world == 1:
+        from pf3d import serve as serve_mod
+        if not args.no_batch:
+            extra["batched"] = bench_batch(args, pf3d, serve_mod, init)
+        if not args.no_serve:
+            extra["serving"] = bench_serve(args, serve_mod)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, n, dt, thr = cpu_oracle_rate(prec, args.cpu_seconds)
@@ -322,6 +396,7 @@ def main():
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk,
     }
+    line.update(extra)
     print(json.dumps(line))
     return 0
 
