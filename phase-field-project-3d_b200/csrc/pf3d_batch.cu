@@ -209,6 +209,15 @@ static int fill_steps(pf_batch* b, BatchStep* rows, int nsteps)
             const double TP_heat = sl.st.TP;
             const double TP = step_tp(p, dt, it, sl.st.TP);
             r.s = make_step_args(p, sl.dv, it, TP_heat, TP, sl.st.M0);
+            if (b->prec == PF_FP64) {
+                KC<double> kc;
+                kc.load(sl.bd.d, r.s);
+                std::memcpy(r.kc, &kc, sizeof(kc));
+            } else {
+                KC<float> kc;
+                kc.load(sl.bd.d, r.s);
+                std::memcpy(r.kc, &kc, sizeof(kc));
+            }
             r.active = 1;
             r.q_phi = sl.qphi;
             r.q_c = sl.qc;

@@ -2,8 +2,9 @@
 //
 // One CTA owns a 32 x TY column tile and a z-chunk and marches along z.  It
 // keeps rolling shared-memory windows:
-//   sphi  : 5 planes of the input phase field with a 2-cell x/y halo
-//           (planes z-2 .. z+2, the next one prefetched with cp.async),
+//   sphi  : 6 planes of the input phase field with a 2-cell x/y halo
+//           (planes z-2 .. z+3; plane z+4 is fetched with cp.async while
+//           plane z is computed, so two planes are always in flight),
 //   snode : 3 planes (z-1, z, z+1) of the anisotropy quantities eps, exy,
 //           eyz, ezx at every node of the tile plus a 1-cell ring
 //           (phase_body.inc:51-129); each is computed once and read by the
@@ -22,9 +23,9 @@
 // per-cell arithmetic is the fast form of pf3d_device.cuh (FAST = true).
 //
 // Latency hiding: the window slots advance incrementally (no modulo), the
-// centre values the cell update reads from global memory (c, DPP) are loaded
-// at the top of the plane iteration, and the concentration values of the
-// next solute plane are loaded one plane ahead into registers.
+// centre values the cell update reads from global memory (c, DPP, T) and the
+// concentration values of the next solute plane are loaded one plane ahead
+// into registers.
 #pragma once
 #include "pf3d_launch.h"
 
@@ -40,13 +41,16 @@ __device__ __forceinline__ void cp_async_elem(void* smem, const void* gmem, int 
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// all but the most recently committed group have landed
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 template <typename T, int TY>
 struct FusedSmem {
     static constexpr int TX = 32;
     static constexpr int PW = TX + 4, PH = TY + 4;   // phase tile with halo 2
     static constexpr int NW = TX + 2, NH = TY + 2;   // node tile with ring 1
-    T phi[5][PH][PW];
+    static constexpr int NS = 6;                     // phase planes z-2 .. z+3
+    T phi[NS][PH][PW];
     T eps[3][NH][NW], exy[3][NH][NW], eyz[3][NH][NW], ezx[3][NH][NW];
     T br[3][NH][NW], mu[3][NH][NW];
 };
@@ -59,13 +63,13 @@ struct FusedOcc {
     static constexpr int v = (warps / TY) > 0 ? (warps / TY) : 1;
 };
 
-__device__ __forceinline__ int add5(int a, int k) { int t = a + k; return t >= 5 ? t - 5 : t; }
+__device__ __forceinline__ int add6(int a, int k) { int t = a + k; return t >= 6 ? t - 6 : t; }
 __device__ __forceinline__ int add3(int a, int k) { int t = a + k; return t >= 3 ? t - 3 : t; }
 
 // One 32 x TY x zchunk tile (tile coordinates bx, by, bz) of one domain.
 // Ends with a CTA-wide barrier, so the caller may reuse the shared memory.
 template <typename T, int TY, bool HEAT, bool DPPW, bool SOL>
-__device__ __forceinline__ void fused_tile(const DomainDesc& d, const StepArgs& s, const T* __restrict__ phi_in,
+__device__ __forceinline__ void fused_tile(const DomainDesc& d, const KC<T>& c, const T* __restrict__ phi_in,
                                            const T* __restrict__ c_in, T* __restrict__ phi_out,
                                            T* __restrict__ dpp, T* __restrict__ c_out,
                                            const T* __restrict__ T_old, T* __restrict__ T_new, int zchunk, int bx,
@@ -85,9 +89,6 @@ __device__ __forceinline__ void fused_tile(const DomainDesc& d, const StepArgs& 
     const int tid = tx + TX * ty;
     const int x = x0 + tx, y = y0 + ty;
     const bool own = (x < nx) && (y < ny);
-
-    KC<T> c;
-    c.load(d, s);
 
     // node-tile position of ring item r: the rows above and below the tile,
     // then the two side columns
@@ -173,8 +174,8 @@ __device__ __forceinline__ void fused_tile(const DomainDesc& d, const StepArgs& 
     };
 
     // ---- prologue: planes zb-2 .. zb+2, nodes zb-1 and zb ----
-    int s5 = zb % 5, s3 = zb % 3;   // window slots of plane zb
-    for (int k = -2; k <= 2; ++k) load_plane(zb + k, add5(s5, (k + 5) % 5));
+    int s5 = zb % 6, s3 = zb % 3;   // window slots of plane zb
+    for (int k = -2; k <= 3; ++k) load_plane(zb + k, add6(s5, (k + 6) % 6));
     cp_async_commit();
     T cpi = 0, cpr = 0, cqi = 0, cqr = 0;   // c of solute planes z+1 (p) and z+2 (q)
     if (SOL) {
@@ -184,20 +185,22 @@ __device__ __forceinline__ void fused_tile(const DomainDesc& d, const StepArgs& 
         load_c(zb + 1, cpi, cpr);
         cp_async_wait_all();
         __syncthreads();
-        sol_plane(zb - 1, add5(s5, 4), add3(s3, 2), ai, ar);
+        sol_plane(zb - 1, add6(s5, 5), add3(s3, 2), ai, ar);
         sol_plane(zb, s5, s3, bi, br_);
     } else {
         cp_async_wait_all();
         __syncthreads();
     }
-    node_plane(zb - 1, add5(s5, 3), add5(s5, 4), s5, add3(s3, 2));
-    node_plane(zb, add5(s5, 4), s5, add5(s5, 1), s3);
+    node_plane(zb - 1, add6(s5, 4), add6(s5, 5), s5, add3(s3, 2));
+    node_plane(zb, add6(s5, 5), s5, add6(s5, 1), s3);
 
     const int fx = tx + 2, fy = ty + 2;   // own cell in the phase tile
     const int nlx = tx + 1, nly = ty + 1; // own cell in the node tile
     const bool xs_src = x >= 1 && x <= nx - 2, ys_src = y >= 1 && y <= ny - 2;
     const bool xs_int = x >= 2 && x <= nx - 3, ys_int = y >= 2 && y <= ny - 3;
     const bool single_xy = x >= 3 && x <= nx - 4 && y >= 3 && y <= ny - 4;
+    // CTA-uniform: every column of the tile is in [3, N-4] in x and y
+    const bool tile_int = x0 >= 3 && x0 + TX + 3 <= nx && y0 >= 3 && y0 + TY + 3 <= ny;
     int xl = 0, xh = -1, yl = 0, yh = -1;
     if (own && xs_src) fpre_range(x, nx, &xl, &xh);
     if (own && ys_src) fpre_range(y, ny, &yl, &yh);
@@ -205,72 +208,104 @@ __device__ __forceinline__ void fused_tile(const DomainDesc& d, const StepArgs& 
     // noise hash input of the own cell, carried along z (k = z + 1)
     uint64_t hin = hash_base(x + 1, y + 1, c.it, 1) + (uint64_t)(zb + 1) * kHashK;
 
+    // centre values of the own cell, one plane ahead
+    T ncpp = 0, ndpp = 0, ntold = 0;
+    if (own && zb < ze) {
+        const long long id0 = col + zoff;
+        ncpp = c_in[id0];
+        if (HEAT) {
+            ndpp = dpp[id0];
+            ntold = T_old[id0];
+        }
+    }
     for (int z = zb; z < ze; ++z, zoff += pl, hin += kHashK) {
         const long long id = col + zoff;
-        // centre values from global memory, consumed after the node pass
-        T cpp = 0, dppv = 0, told = 0;
-        if (own) {
-            cpp = c_in[id];
+        const T cpp = ncpp, dppv = ndpp, told = ntold;
+        if (own && z + 1 < ze) {
+            ncpp = c_in[id + pl];
             if (HEAT) {
-                dppv = dpp[id];
-                told = T_old[id];
+                ndpp = dpp[id + pl];
+                ntold = T_old[id + pl];
             }
         }
         if (SOL) load_c(z + 2, cqi, cqr);
-        node_plane(z + 1, s5, add5(s5, 1), add5(s5, 2), add3(s3, 1));
-        if (SOL) sol_plane(z + 1, add5(s5, 1), add3(s3, 1), cpi, cpr);
+        node_plane(z + 1, s5, add6(s5, 1), add6(s5, 2), add3(s3, 1));
+        if (SOL) sol_plane(z + 1, add6(s5, 1), add3(s3, 1), cpi, cpr);
         __syncthreads();
-        load_plane(z + 3, add5(s5, 3));
+        load_plane(z + 4, add6(s5, 4));
         cp_async_commit();
 
-        if (own) {
-            const T(*pm)[PW] = sm.phi[add5(s5, 4)];
-            const T(*p0)[PW] = sm.phi[s5];
-            const T(*pp)[PW] = sm.phi[add5(s5, 1)];
-            const int n0 = s3, np1 = add3(s3, 1), nm1 = add3(s3, 2);
+        const T(*pm)[PW] = sm.phi[add6(s5, 5)];
+        const T(*p0)[PW] = sm.phi[s5];
+        const T(*pp)[PW] = sm.phi[add6(s5, 1)];
+        const int n0 = s3, np1 = add3(s3, 1), nm1 = add3(s3, 2);
+
+        // phase_body.inc at the own cell: PPNEW
+        auto phase_cell = [&](T PPc, T cpp, int z) -> T {
+            Nbr<T> nb;
+            nb.PP = PPc;
+            nb.PN = p0[fy + 1][fx]; nb.PS = p0[fy - 1][fx];
+            nb.PE = p0[fy][fx + 1]; nb.PW = p0[fy][fx - 1];
+            nb.PT = pp[fy][fx]; nb.PB = pm[fy][fx];
+            nb.PNE = p0[fy + 1][fx + 1]; nb.PSE = p0[fy - 1][fx + 1];
+            nb.PNW = p0[fy + 1][fx - 1]; nb.PSW = p0[fy - 1][fx - 1];
+            nb.PNT = pp[fy + 1][fx]; nb.PNB = pm[fy + 1][fx];
+            nb.PST = pp[fy - 1][fx]; nb.PSB = pm[fy - 1][fx];
+            nb.PET = pp[fy][fx + 1]; nb.PEB = pm[fy][fx + 1];
+            nb.PWT = pp[fy][fx - 1]; nb.PWB = pm[fy][fx - 1];
+            Node<T> E, W, N, S, Tt, B;
+            E.eps = sm.eps[n0][nly][nlx + 1]; E.exy = sm.exy[n0][nly][nlx + 1]; E.ezx = sm.ezx[n0][nly][nlx + 1];
+            W.eps = sm.eps[n0][nly][nlx - 1]; W.exy = sm.exy[n0][nly][nlx - 1]; W.ezx = sm.ezx[n0][nly][nlx - 1];
+            N.eps = sm.eps[n0][nly + 1][nlx]; N.exy = sm.exy[n0][nly + 1][nlx]; N.eyz = sm.eyz[n0][nly + 1][nlx];
+            S.eps = sm.eps[n0][nly - 1][nlx]; S.exy = sm.exy[n0][nly - 1][nlx]; S.eyz = sm.eyz[n0][nly - 1][nlx];
+            Tt.eps = sm.eps[np1][nly][nlx]; Tt.eyz = sm.eyz[np1][nly][nlx]; Tt.ezx = sm.ezx[np1][nly][nlx];
+            B.eps = sm.eps[nm1][nly][nlx]; B.eyz = sm.eyz[nm1][nly][nlx]; B.ezx = sm.ezx[nm1][nly][nlx];
+            E.eyz = W.eyz = N.ezx = S.ezx = Tt.exy = B.exy = (T)0;   // unused by the body
+            const float ran = (c.rt == 2) ? phase_ran(2, x + 1, y + 1, z + 1, c.it)
+                                          : __double2float_rn(ran64(hash63_mix(hin)));
+            return phase_ppnew<T, true>(nb, E, W, N, S, Tt, B, cpp, ran, c);
+        };
+        // conc_body.inc at the own cell
+        auto solute_cell = [&](T PPc, T cpp) -> T {
+            SolNode<T> nP{sm.br[n0][nly][nlx], sm.mu[n0][nly][nlx]};
+            SolNode<T> nE{sm.br[n0][nly][nlx + 1], sm.mu[n0][nly][nlx + 1]};
+            SolNode<T> nW{sm.br[n0][nly][nlx - 1], sm.mu[n0][nly][nlx - 1]};
+            SolNode<T> nN{sm.br[n0][nly + 1][nlx], sm.mu[n0][nly + 1][nlx]};
+            SolNode<T> nS{sm.br[n0][nly - 1][nlx], sm.mu[n0][nly - 1][nlx]};
+            SolNode<T> nT{sm.br[np1][nly][nlx], sm.mu[np1][nly][nlx]};
+            SolNode<T> nB{sm.br[nm1][nly][nlx], sm.mu[nm1][nly][nlx]};
+            return conc_new<T, true>(PPc, cpp, nP, nE, nW, nN, nS, nT, nB, c);
+        };
+        auto heat_cell = [&](T PPc, T dppv) -> T {
+            T TE = 0, TW = 0, TN = 0, TS = 0, TT = 0, TB = 0;
+            if (c.lap) {
+                TE = T_old[id + 1]; TW = T_old[id - 1]; TN = T_old[id + px]; TS = T_old[id - px];
+                TT = T_old[id + pl]; TB = T_old[id - pl];
+            }
+            return heat_new<T>(PPc, dppv, TE, TW, TN, TS, TT, TB, c);
+        };
+
+        if (tile_int && z >= 3 && z <= nz - 4) {
+            // the whole tile plane is interior and every cell is its own only
+            // preimage: no bounds, decoration or scatter (CTA-uniform branch)
+            const T PPc = p0[fy][fx];
+            if (HEAT) T_new[id] = heat_cell(PPc, dppv);
+            const T ppn = phase_cell(PPc, cpp, z);
+            if (DPPW) dpp[id] = ppn - PPc;
+            phi_out[id] = clamp01(ppn);
+            if (SOL) c_out[id] = solute_cell(PPc, cpp);
+        } else if (own) {
             const T PPc = p0[fy][fx];
             const bool zin = z >= 1 && z <= nz - 2;
 
             // ---- temperatura ----
-            if (HEAT) {
-                if (xs_src && ys_src && zin) {
-                    T TE = 0, TW = 0, TN = 0, TS = 0, TT = 0, TB = 0;
-                    if (c.lap) {
-                        TE = T_old[id + 1]; TW = T_old[id - 1]; TN = T_old[id + px]; TS = T_old[id - px];
-                        TT = T_old[id + pl]; TB = T_old[id - pl];
-                    }
-                    T_new[id] = heat_new<T>(PPc, dppv, TE, TW, TN, TS, TT, TB, c);
-                } else {
-                    T_new[id] = told;
-                }
-            }
+            if (HEAT) T_new[id] = (xs_src && ys_src && zin) ? heat_cell(PPc, dppv) : told;
 
             // ---- phase sweep ----
             if (xs_src && ys_src && zin) {
                 T U;
                 if (xs_int && ys_int && z >= 2 && z <= nz - 3) {
-                    Nbr<T> nb;
-                    nb.PP = PPc;
-                    nb.PN = p0[fy + 1][fx]; nb.PS = p0[fy - 1][fx];
-                    nb.PE = p0[fy][fx + 1]; nb.PW = p0[fy][fx - 1];
-                    nb.PT = pp[fy][fx]; nb.PB = pm[fy][fx];
-                    nb.PNE = p0[fy + 1][fx + 1]; nb.PSE = p0[fy - 1][fx + 1];
-                    nb.PNW = p0[fy + 1][fx - 1]; nb.PSW = p0[fy - 1][fx - 1];
-                    nb.PNT = pp[fy + 1][fx]; nb.PNB = pm[fy + 1][fx];
-                    nb.PST = pp[fy - 1][fx]; nb.PSB = pm[fy - 1][fx];
-                    nb.PET = pp[fy][fx + 1]; nb.PEB = pm[fy][fx + 1];
-                    nb.PWT = pp[fy][fx - 1]; nb.PWB = pm[fy][fx - 1];
-                    Node<T> E, W, N, S, Tt, B;
-                    E.eps = sm.eps[n0][nly][nlx + 1]; E.exy = sm.exy[n0][nly][nlx + 1]; E.ezx = sm.ezx[n0][nly][nlx + 1];
-                    W.eps = sm.eps[n0][nly][nlx - 1]; W.exy = sm.exy[n0][nly][nlx - 1]; W.ezx = sm.ezx[n0][nly][nlx - 1];
-                    N.eps = sm.eps[n0][nly + 1][nlx]; N.exy = sm.exy[n0][nly + 1][nlx]; N.eyz = sm.eyz[n0][nly + 1][nlx];
-                    S.eps = sm.eps[n0][nly - 1][nlx]; S.exy = sm.exy[n0][nly - 1][nlx]; S.eyz = sm.eyz[n0][nly - 1][nlx];
-                    Tt.eps = sm.eps[np1][nly][nlx]; Tt.eyz = sm.eyz[np1][nly][nlx]; Tt.ezx = sm.ezx[np1][nly][nlx];
-                    B.eps = sm.eps[nm1][nly][nlx]; B.eyz = sm.eyz[nm1][nly][nlx]; B.ezx = sm.ezx[nm1][nly][nlx];
-                    E.eyz = W.eyz = N.ezx = S.ezx = Tt.exy = B.exy = (T)0;   // unused by the body
-                    float ran = (c.rt == 2) ? phase_ran(2, x + 1, y + 1, z + 1, c.it)
-                                            : __double2float_rn(ran64(hash63_mix(hin)));
-                    T ppn = phase_ppnew<T, true>(nb, E, W, N, S, Tt, B, cpp, ran, c);
+                    const T ppn = phase_cell(PPc, cpp, z);
                     if (DPPW) dpp[id] = ppn - PPc;
                     U = clamp01(ppn);
                 } else {
@@ -295,14 +330,7 @@ __device__ __forceinline__ void fused_tile(const DomainDesc& d, const StepArgs& 
                 if (feeds) {
                     T Uc;
                     if (inner) {
-                        SolNode<T> nP{sm.br[n0][nly][nlx], sm.mu[n0][nly][nlx]};
-                        SolNode<T> nE{sm.br[n0][nly][nlx + 1], sm.mu[n0][nly][nlx + 1]};
-                        SolNode<T> nW{sm.br[n0][nly][nlx - 1], sm.mu[n0][nly][nlx - 1]};
-                        SolNode<T> nN{sm.br[n0][nly + 1][nlx], sm.mu[n0][nly + 1][nlx]};
-                        SolNode<T> nS{sm.br[n0][nly - 1][nlx], sm.mu[n0][nly - 1][nlx]};
-                        SolNode<T> nT{sm.br[np1][nly][nlx], sm.mu[np1][nly][nlx]};
-                        SolNode<T> nB{sm.br[nm1][nly][nlx], sm.mu[nm1][nly][nlx]};
-                        Uc = conc_new<T, true>(PPc, cpp, nP, nE, nW, nN, nS, nT, nB, c);
+                        Uc = solute_cell(PPc, cpp);
                         c_out[id] = Uc;
                     } else {
                         Uc = cpp;
@@ -317,23 +345,24 @@ __device__ __forceinline__ void fused_tile(const DomainDesc& d, const StepArgs& 
             }
         }
         if (SOL) { cpi = cqi; cpr = cqr; }
-        cp_async_wait_all();
+        cp_async_wait_prev();   // plane z+3 (needed next) has landed; z+4 may be in flight
         __syncthreads();
-        s5 = add5(s5, 1);
+        s5 = add6(s5, 1);
         s3 = add3(s3, 1);
     }
+    cp_async_wait_all();
     __syncthreads();
 }
 
 // single domain: one CTA per tile
 template <typename T, int TY, bool HEAT, bool DPPW, bool SOL>
 __global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY>::v))
-    k_fused(DomainDesc d, StepArgs s, const T* __restrict__ phi_in, const T* __restrict__ c_in,
+    k_fused(DomainDesc d, const KC<T> c, const T* __restrict__ phi_in, const T* __restrict__ c_in,
             T* __restrict__ phi_out, T* __restrict__ dpp, T* __restrict__ c_out, const T* __restrict__ T_old,
             T* __restrict__ T_new, int zchunk)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    fused_tile<T, TY, HEAT, DPPW, SOL>(d, s, phi_in, c_in, phi_out, dpp, c_out, T_old, T_new, zchunk, blockIdx.x,
+    fused_tile<T, TY, HEAT, DPPW, SOL>(d, c, phi_in, c_in, phi_out, dpp, c_out, T_old, T_new, zchunk, blockIdx.x,
                                        blockIdx.y, blockIdx.z, smem_raw);
 }
 
@@ -346,24 +375,31 @@ __global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY>::v))
                   const BatchItem* __restrict__ items, const int* __restrict__ n_items, int zchunk)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(16) KC<T> skc;   // the loop constants of the current item
     const int n = *n_items;
+    const int tid = threadIdx.x + 32 * threadIdx.y;
     for (int w = blockIdx.x; w < n; w += gridDim.x) {
         const BatchItem it = items[w];
         const BatchStep& st = steps[it.dom];
         if (!st.active) continue;   // uniform across the CTA
         const BatchDomain& D = doms[it.dom];
         const int q = st.q_phi, qc = st.q_c, qt = st.q_T;
+        static_assert(sizeof(KC<T>) % 4 == 0, "KC is copied as words");
+        if (tid < (int)(sizeof(KC<T>) / 4))
+            reinterpret_cast<int*>(&skc)[tid] = reinterpret_cast<const int*>(st.kc)[tid];
+        __syncthreads();
+        const KC<T>& kc = skc;
         if (PASS == 0) {
             if (ONE_SWEEP)
-                fused_tile<T, TY, true, true, true>(D.d, st.s, (const T*)D.phi[q], (const T*)D.c[qc], (T*)D.phi[1 - q],
+                fused_tile<T, TY, true, true, true>(D.d, kc, (const T*)D.phi[q], (const T*)D.c[qc], (T*)D.phi[1 - q],
                                                     (T*)D.dpp, (T*)D.c[1 - qc], (const T*)D.T[qt], (T*)D.T[1 - qt],
                                                     zchunk, it.bx, it.by, it.bz, smem_raw);
             else
-                fused_tile<T, TY, true, false, false>(D.d, st.s, (const T*)D.phi[q], (const T*)D.c[qc],
+                fused_tile<T, TY, true, false, false>(D.d, kc, (const T*)D.phi[q], (const T*)D.c[qc],
                                                       (T*)D.phi[1 - q], (T*)D.dpp, nullptr, (const T*)D.T[qt],
                                                       (T*)D.T[1 - qt], zchunk, it.bx, it.by, it.bz, smem_raw);
         } else {
-            fused_tile<T, TY, false, true, true>(D.d, st.s, (const T*)D.phi[1 - q], (const T*)D.c[qc], (T*)D.phi[q],
+            fused_tile<T, TY, false, true, true>(D.d, kc, (const T*)D.phi[1 - q], (const T*)D.c[qc], (T*)D.phi[q],
                                                  (T*)D.dpp, (T*)D.c[1 - qc], nullptr, nullptr, zchunk, it.bx, it.by,
                                                  it.bz, smem_raw);
         }
@@ -390,8 +426,10 @@ cudaError_t launch_fused_t(const DomainDesc& d, const StepArgs& s, const void* p
         configured = true;
     }
     if (zchunk <= 0) zchunk = d.nz;
+    KC<T> kc;
+    kc.load(d, s);
     dim3 grid((d.nx + 31) / 32, (d.ny + TY - 1) / TY, (d.nz + zchunk - 1) / zchunk);
-    kern<<<grid, dim3(32, TY), smem, st>>>(d, s, (const T*)phi_in, (const T*)c_in, (T*)phi_out, (T*)dpp, (T*)c_out,
+    kern<<<grid, dim3(32, TY), smem, st>>>(d, kc, (const T*)phi_in, (const T*)c_in, (T*)phi_out, (T*)dpp, (T*)c_out,
                                            (const T*)T_old, (T*)T_new, zchunk);
     return cudaGetLastError();
 }

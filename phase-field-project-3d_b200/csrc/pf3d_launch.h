@@ -50,6 +50,9 @@ struct BatchStep {
     StepArgs s;
     int active;
     int q_phi, q_c, q_T;
+    int pad_;
+    // the loop constants of this domain and step, KC<T> of the batch's type
+    alignas(16) unsigned char kc[sizeof(KC<double>)];
 };
 struct BatchItem {
     int dom, bx, by, bz;
