@@ -263,16 +263,11 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
+    from pf3d import replicas
+    barrier = replicas.barrier
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, device="cuda")
 
     w = deck.WORKLOADS[args.workload]
     g, p = w.grid(), w.params()
@@ -302,7 +297,7 @@ def main():
     barrier()
     ms = max_over_ranks(e0.elapsed_time(e1))
     clk = clocks.stop()
-    value = cells * args.steps * world / (ms / 1e3) / 1e9
+    value = replicas.aggregate_rate(cells, args.steps, world, ms / 1e3)
     launches_per_step = 2 if p.n_varreduras >= 2 else 1
     launches_per_step += max(0, p.n_varreduras - 2)
 
