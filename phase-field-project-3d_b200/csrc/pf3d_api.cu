@@ -465,8 +465,9 @@ static int one_step(pf_ctx* ctx)
             void* cur = B;   // phase after the sweeps so far
             void* oth = A;   // free buffer
             for (int sw = 2; sw <= nsw - 1; ++sw) {
-                CK(is64(ctx) ? launch_phase<double>(ctx->dd, s, cur, f.c_old, oth, f.dpp, ctx->stream)
-                             : launch_phase<float>(ctx->dd, s, cur, f.c_old, oth, f.dpp, ctx->stream),
+                // no DPP: it carries the step's noise from the first to the last pass
+                CK(is64(ctx) ? launch_phase<double>(ctx->dd, s, cur, f.c_old, oth, nullptr, ctx->stream)
+                             : launch_phase<float>(ctx->dd, s, cur, f.c_old, oth, nullptr, ctx->stream),
                    "middle sweep");
                 std::swap(cur, oth);
             }

@@ -18,6 +18,11 @@
 //   HEAT : temperatura (TNEW from TOLD, DPP and the centre phase value)
 //   DPPW : write DPP (only the last sweep of a step needs to)
 //   SOL  : concentracao_soluto from the same input phase field
+// Noise: every sweep of a step draws the same noise (same it), so the first
+//   pass of a multi-sweep step stores the REAL(4) ran of every interior cell
+//   in the DPP buffer after the heat equation has read that cell's DPP, and
+//   the last pass reads it back before writing the new DPP (sweeps in between
+//   leave DPP alone); a single-sweep pass draws it.
 // Every output is written with the closed-form boundary decoration, so one
 // pass replaces the reference's copy + stencil + plane-copy kernels.  The
 // per-cell arithmetic is the fast form of pf3d_device.cuh (FAST = true).
@@ -78,6 +83,8 @@ __device__ __forceinline__ void fused_tile(const DomainDesc& d, const KC<T>& c, 
     using SM = FusedSmem<T, TY>;
     constexpr int TX = SM::TX, PW = SM::PW, PH = SM::PH, NW = SM::NW, NH = SM::NH;
     constexpr int RING = 2 * NW + 2 * TY;   // ring nodes around the tile
+    // noise hand-over: first pass of a multi-sweep step stores, last reads
+    constexpr int ran_mode = (HEAT && !DPPW) ? 1 : ((!HEAT && DPPW) ? 2 : 0);
     SM& sm = *reinterpret_cast<SM*>(smem_raw);
 
     const int nx = d.nx, ny = d.ny, nz = d.nz;
@@ -216,6 +223,8 @@ __device__ __forceinline__ void fused_tile(const DomainDesc& d, const KC<T>& c, 
         if (HEAT) {
             ndpp = dpp[id0];
             ntold = T_old[id0];
+        } else if (ran_mode == 2) {
+            ndpp = dpp[id0];
         }
     }
     for (int z = zb; z < ze; ++z, zoff += pl, hin += kHashK) {
@@ -226,6 +235,8 @@ __device__ __forceinline__ void fused_tile(const DomainDesc& d, const KC<T>& c, 
             if (HEAT) {
                 ndpp = dpp[id + pl];
                 ntold = T_old[id + pl];
+            } else if (ran_mode == 2) {
+                ndpp = dpp[id + pl];
             }
         }
         if (SOL) load_c(z + 2, cqi, cqr);
@@ -261,8 +272,14 @@ __device__ __forceinline__ void fused_tile(const DomainDesc& d, const KC<T>& c, 
             Tt.eps = sm.eps[np1][nly][nlx]; Tt.eyz = sm.eyz[np1][nly][nlx]; Tt.ezx = sm.ezx[np1][nly][nlx];
             B.eps = sm.eps[nm1][nly][nlx]; B.eyz = sm.eyz[nm1][nly][nlx]; B.ezx = sm.ezx[nm1][nly][nlx];
             E.eyz = W.eyz = N.ezx = S.ezx = Tt.exy = B.exy = (T)0;   // unused by the body
-            const float ran = (c.rt == 2) ? phase_ran(2, x + 1, y + 1, z + 1, c.it)
-                                          : __double2float_rn(ran64(hash63_mix(hin)));
+            float ran;
+            if constexpr (ran_mode == 2) {
+                ran = (float)dppv;   // drawn and stored by the first pass
+            } else {
+                ran = (c.rt == 2) ? phase_ran(2, x + 1, y + 1, z + 1, c.it)
+                                  : __double2float_rn(ran64(hash63_mix(hin)));
+                if constexpr (ran_mode == 1) dpp[id] = (T)ran;
+            }
             return phase_ppnew<T, true>(nb, E, W, N, S, Tt, B, cpp, ran, c);
         };
         // conc_body.inc at the own cell

@@ -31,6 +31,8 @@ template <typename T> cudaError_t launch_copy_inner(const DomainDesc& d, const v
 //   first  : temperatura + phase sweep 1 (phi_old -> phi_mid), or with
 //            solute as well when there is a single sweep
 //   last   : final phase sweep (phi_mid -> phi_new) + solute from phi_mid
+//   The first pass of a multi-sweep step leaves the step's noise in the DPP
+//   buffer for the last pass; sweeps in between must not write DPP.
 template <typename T> cudaError_t launch_fused_first(const DomainDesc& d, const StepArgs& s, const Fields& f,
                                                      bool with_solute, int tile_y, int zchunk, cudaStream_t st);
 template <typename T> cudaError_t launch_fused_last(const DomainDesc& d, const StepArgs& s, const Fields& f,

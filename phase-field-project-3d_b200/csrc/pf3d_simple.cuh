@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(256) k_phase(DomainDesc d, StepArgs s, const T
                                   grad<T, FAST>(nb.PP, P(0, 0, -2), c.dz, c.hz), c);
         float ran = phase_ran(c.rt, x + 1, y + 1, z + 1, c.it);
         T ppn = phase_ppnew<T, FAST>(nb, E, W, N, S, Tt, B, co[id], ran, c);
-        dpp[id] = ppn - nb.PP;
+        if (dpp) dpp[id] = ppn - nb.PP;   // the fused step's middle sweeps pass no DPP
         U = clamp01(ppn);
     } else {
         U = po[id];
