@@ -76,10 +76,10 @@ struct pf_batch {
     double* d_part = nullptr;          // diagnostics partials (592 x 8) + result
     double* h_out = nullptr;
     double* d_sites = nullptr;         // bump sites for device initialisation
-    int tile_y = 8, zchunk = 64, grid = 0;
+    int tile_y = 8, zchunk = 64, n_sm = 0;   // persistent grids: n_sm x resident CTAs
     cudaStream_t own_stream = nullptr, stream = nullptr;
     cudaGraphExec_t graph = nullptr;
-    int graph_ty = 0, graph_zc = 0, graph_grid = 0, graph_nsw = 0;
+    int graph_ty = 0, graph_zc = 0, graph_nsm = 0, graph_nsw = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
     long long last_steps = 0;
@@ -141,7 +141,7 @@ static int rebuild_items(pf_batch* b)
 
 static int capture_graph(pf_batch* b)
 {
-    if (b->graph && b->graph_ty == b->tile_y && b->graph_zc == b->zchunk && b->graph_grid == b->grid &&
+    if (b->graph && b->graph_ty == b->tile_y && b->graph_zc == b->zchunk && b->graph_nsm == b->n_sm &&
         b->graph_nsw == b->nsw)
         return PF_OK;
     if (b->graph) {
@@ -157,14 +157,14 @@ static int capture_graph(pf_batch* b)
             const BatchStep* st = b->d_steps + (size_t)k * b->max_domains;
             const bool one = b->nsw == 1;
             e = b64(b) ? launch_fused_batch<double>(b->d_doms, st, b->d_items, b->d_nitems, 0, one, b->tile_y, b->zchunk,
-                                                    b->grid, cs)
+                                                    b->n_sm, cs)
                        : launch_fused_batch<float>(b->d_doms, st, b->d_items, b->d_nitems, 0, one, b->tile_y, b->zchunk,
-                                                   b->grid, cs);
+                                                   b->n_sm, cs);
             if (e == cudaSuccess && !one)
                 e = b64(b) ? launch_fused_batch<double>(b->d_doms, st, b->d_items, b->d_nitems, 1, false, b->tile_y,
-                                                        b->zchunk, b->grid, cs)
+                                                        b->zchunk, b->n_sm, cs)
                            : launch_fused_batch<float>(b->d_doms, st, b->d_items, b->d_nitems, 1, false, b->tile_y,
-                                                       b->zchunk, b->grid, cs);
+                                                       b->zchunk, b->n_sm, cs);
         }
         cudaError_t e2 = cudaStreamEndCapture(cs, &g);
         if (e == cudaSuccess) e = e2;
@@ -175,7 +175,7 @@ static int capture_graph(pf_batch* b)
     if (e != cudaSuccess) return berr(b, PF_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
     b->graph_ty = b->tile_y;
     b->graph_zc = b->zchunk;
-    b->graph_grid = b->grid;
+    b->graph_nsm = b->n_sm;
     b->graph_nsw = b->nsw;
     return PF_OK;
 }
@@ -185,8 +185,7 @@ static int set_grid(pf_batch* b)
     int dev = 0, nsm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const int per = b64(b) ? batch_blocks_per_sm<double>(b->tile_y) : batch_blocks_per_sm<float>(b->tile_y);
-    b->grid = std::max(1, nsm) * per;
+    b->n_sm = std::max(1, nsm);
     return PF_OK;
 }
 

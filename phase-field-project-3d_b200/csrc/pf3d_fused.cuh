@@ -60,11 +60,13 @@ struct FusedSmem {
     T br[3][NH][NW], mu[3][NH][NW];
 };
 
-// resident CTAs per SM the register budget is sized for: 16 warps in FP64,
-// 24 in FP32
-template <typename T, int TY>
+// resident CTAs per SM the register budget is sized for.  K = 0: passes with
+// the heat equation (they need about 128 registers a thread in FP64 and slow
+// down sharply when squeezed), K = 1: the last pass (fits 80 registers in
+// FP64 without spills, so 24 warps).  FP32 runs 24 warps in both.
+template <typename T, int TY, int K>
 struct FusedOcc {
-    static constexpr int warps = (sizeof(T) == 8) ? 16 : 24;
+    static constexpr int warps = (sizeof(T) == 8) ? (K == 0 ? 16 : 24) : 24;
     static constexpr int v = (warps / TY) > 0 ? (warps / TY) : 1;
 };
 
@@ -373,7 +375,7 @@ __device__ __forceinline__ void fused_tile(const DomainDesc& d, const KC<T>& c, 
 
 // single domain: one CTA per tile
 template <typename T, int TY, bool HEAT, bool DPPW, bool SOL>
-__global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY>::v))
+__global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY, HEAT ? 0 : 1>::v))
     k_fused(DomainDesc d, const KC<T> c, const T* __restrict__ phi_in, const T* __restrict__ c_in,
             T* __restrict__ phi_out, T* __restrict__ dpp, T* __restrict__ c_out, const T* __restrict__ T_old,
             T* __restrict__ T_new, int zchunk)
@@ -387,7 +389,7 @@ __global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY>::v))
 // pass of a step (temperatura + sweep 1, or the whole step with one sweep),
 // PASS 1 the last (sweep 2 + solute).
 template <typename T, int TY, int PASS, bool ONE_SWEEP>
-__global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY>::v))
+__global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY, PASS == 0 ? 0 : 1>::v))
     k_fused_batch(const BatchDomain* __restrict__ doms, const BatchStep* __restrict__ steps,
                   const BatchItem* __restrict__ items, const int* __restrict__ n_items, int zchunk)
 {
@@ -485,58 +487,44 @@ cudaError_t launch_fused_last(const DomainDesc& d, const StepArgs& s, const Fiel
                                                  tile_y, zchunk, st);
 }
 
+// The persistent grid is the SM count times the CTAs of this kernel that are
+// resident on one SM (each pass has its own register budget).
 template <typename T, int TY, int PASS, bool ONE_SWEEP>
 cudaError_t launch_batch_t(const BatchDomain* doms, const BatchStep* steps, const BatchItem* items, const int* n_items,
-                           int zchunk, int grid, cudaStream_t st)
+                           int zchunk, int n_sm, cudaStream_t st)
 {
     auto kern = k_fused_batch<T, TY, PASS, ONE_SWEEP>;
     const size_t smem = fused_smem_bytes<T, TY>();
-    static bool configured = false;
-    if (!configured) {
+    static int per_sm = 0;   // one attribute and occupancy query per instantiation
+    if (per_sm == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        configured = true;
+        int nb = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 32 * TY, smem);
+        if (e != cudaSuccess) return e;
+        per_sm = nb > 0 ? nb : 1;
     }
-    kern<<<grid, dim3(32, TY), smem, st>>>(doms, steps, items, n_items, zchunk);
+    kern<<<n_sm * per_sm, dim3(32, TY), smem, st>>>(doms, steps, items, n_items, zchunk);
     return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_fused_batch(const BatchDomain* doms, const BatchStep* steps, const BatchItem* items,
-                               const int* n_items, int pass, bool one_sweep, int tile_y, int zchunk, int grid,
+                               const int* n_items, int pass, bool one_sweep, int tile_y, int zchunk, int n_sm,
                                cudaStream_t st)
 {
 #define PF3D_BATCH_CASE(TYV)                                                                                   \
     if (tile_y == TYV) {                                                                                       \
         if (pass == 0)                                                                                         \
-            return one_sweep ? launch_batch_t<T, TYV, 0, true>(doms, steps, items, n_items, zchunk, grid, st)  \
-                             : launch_batch_t<T, TYV, 0, false>(doms, steps, items, n_items, zchunk, grid, st); \
-        return launch_batch_t<T, TYV, 1, false>(doms, steps, items, n_items, zchunk, grid, st);               \
+            return one_sweep ? launch_batch_t<T, TYV, 0, true>(doms, steps, items, n_items, zchunk, n_sm, st)  \
+                             : launch_batch_t<T, TYV, 0, false>(doms, steps, items, n_items, zchunk, n_sm, st); \
+        return launch_batch_t<T, TYV, 1, false>(doms, steps, items, n_items, zchunk, n_sm, st);               \
     }
     PF3D_BATCH_CASE(4)
     PF3D_BATCH_CASE(16)
     PF3D_BATCH_CASE(8)
 #undef PF3D_BATCH_CASE
     return cudaErrorInvalidValue;
-}
-
-template <typename T>
-int batch_blocks_per_sm(int tile_y)
-{
-    int nb = 0;
-    const void* fn = nullptr;
-    size_t smem = 0;
-    switch (tile_y) {
-    case 4: fn = (const void*)k_fused_batch<T, 4, 1, false>; smem = fused_smem_bytes<T, 4>(); break;
-    case 16: fn = (const void*)k_fused_batch<T, 16, 1, false>; smem = fused_smem_bytes<T, 16>(); break;
-    default: fn = (const void*)k_fused_batch<T, 8, 1, false>; smem = fused_smem_bytes<T, 8>(); break;
-    }
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, 32 * tile_y, smem) != cudaSuccess) {
-        cudaGetLastError();
-        return 1;
-    }
-    return nb > 0 ? nb : 1;
 }
 
 }  // namespace pf3d

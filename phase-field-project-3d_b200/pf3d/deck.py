@@ -159,4 +159,8 @@ WORKLOADS = {
     "c3_1024cube_fp32": Workload("c3_1024cube_fp32", 1024, 1024, 1024, 0.5e-6, 10000, 2, 256, 32, dict(_COMMON)),
     "c3_replica_256x256x512_fp64": Workload("c3_replica_256x256x512_fp64", 256, 256, 512, 0.5e-6, 10000, 2, 16, 64,
                                              dict(_COMMON)),
+    # profiling cases: the same kernels on a state still larger than L2
+    # (4 fields x 16.8M cells = 537 MB in FP64, 268 MB in FP32)
+    "ncu_256x256x256_fp64": Workload("ncu_256x256x256_fp64", 256, 256, 256, 0.5e-6, 5, 1, 16, 64, dict(_COMMON)),
+    "ncu_256x256x256_fp32": Workload("ncu_256x256x256_fp32", 256, 256, 256, 0.5e-6, 5, 1, 16, 32, dict(_COMMON)),
 }
