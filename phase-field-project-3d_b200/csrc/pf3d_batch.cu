@@ -80,6 +80,7 @@ struct pf_batch {
     cudaStream_t own_stream = nullptr, stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graph_ty = 0, graph_zc = 0, graph_nsm = 0, graph_nsw = 0;
+    bool graph_smooth = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
     long long last_steps = 0;
@@ -139,10 +140,20 @@ static int rebuild_items(pf_batch* b)
     return PF_OK;
 }
 
+// whether any domain of the batch draws the smooth noise (ruido_tipo 2): the
+// first-pass kernels carry that code only when one does
+static bool any_smooth(const pf_batch* b)
+{
+    for (const Slot& sl : b->slots)
+        if (sl.used && sl.p.ruido_tipo == 2) return true;
+    return false;
+}
+
 static int capture_graph(pf_batch* b)
 {
+    const bool smooth = any_smooth(b);
     if (b->graph && b->graph_ty == b->tile_y && b->graph_zc == b->zchunk && b->graph_nsm == b->n_sm &&
-        b->graph_nsw == b->nsw)
+        b->graph_nsw == b->nsw && b->graph_smooth == smooth)
         return PF_OK;
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
@@ -156,15 +167,15 @@ static int capture_graph(pf_batch* b)
         for (int k = 0; k < kGraphSteps && e == cudaSuccess; ++k) {
             const BatchStep* st = b->d_steps + (size_t)k * b->max_domains;
             const bool one = b->nsw == 1;
-            e = b64(b) ? launch_fused_batch<double>(b->d_doms, st, b->d_items, b->d_nitems, 0, one, b->tile_y, b->zchunk,
-                                                    b->n_sm, cs)
-                       : launch_fused_batch<float>(b->d_doms, st, b->d_items, b->d_nitems, 0, one, b->tile_y, b->zchunk,
-                                                   b->n_sm, cs);
+            e = b64(b) ? launch_fused_batch<double>(b->d_doms, st, b->d_items, b->d_nitems, 0, one, smooth, b->tile_y,
+                                                    b->zchunk, b->n_sm, cs)
+                       : launch_fused_batch<float>(b->d_doms, st, b->d_items, b->d_nitems, 0, one, smooth, b->tile_y,
+                                                   b->zchunk, b->n_sm, cs);
             if (e == cudaSuccess && !one)
-                e = b64(b) ? launch_fused_batch<double>(b->d_doms, st, b->d_items, b->d_nitems, 1, false, b->tile_y,
-                                                        b->zchunk, b->n_sm, cs)
-                           : launch_fused_batch<float>(b->d_doms, st, b->d_items, b->d_nitems, 1, false, b->tile_y,
-                                                       b->zchunk, b->n_sm, cs);
+                e = b64(b) ? launch_fused_batch<double>(b->d_doms, st, b->d_items, b->d_nitems, 1, false, false,
+                                                        b->tile_y, b->zchunk, b->n_sm, cs)
+                           : launch_fused_batch<float>(b->d_doms, st, b->d_items, b->d_nitems, 1, false, false,
+                                                       b->tile_y, b->zchunk, b->n_sm, cs);
         }
         cudaError_t e2 = cudaStreamEndCapture(cs, &g);
         if (e == cudaSuccess) e = e2;
@@ -177,6 +188,7 @@ static int capture_graph(pf_batch* b)
     b->graph_zc = b->zchunk;
     b->graph_nsm = b->n_sm;
     b->graph_nsw = b->nsw;
+    b->graph_smooth = smooth;
     return PF_OK;
 }
 

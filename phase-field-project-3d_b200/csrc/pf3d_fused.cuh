@@ -60,13 +60,14 @@ struct FusedSmem {
     T br[3][NH][NW], mu[3][NH][NW];
 };
 
-// resident CTAs per SM the register budget is sized for.  K = 0: passes with
-// the heat equation (they need about 128 registers a thread in FP64 and slow
-// down sharply when squeezed), K = 1: the last pass (fits 80 registers in
-// FP64 without spills, so 24 warps).  FP32 runs 24 warps in both.
+// resident CTAs per SM the register budget is sized for.  K = 1: a pass that
+// draws the smooth noise (ruido_tipo 2) inline; its trilinear blend of eight
+// hashes needs about 128 registers a thread in FP64, which caps it at 16
+// warps.  K = 0: every other pass fits 80 registers without spills, so 24
+// warps.  FP32 runs 24 warps in both.
 template <typename T, int TY, int K>
 struct FusedOcc {
-    static constexpr int warps = (sizeof(T) == 8) ? (K == 0 ? 16 : 24) : 24;
+    static constexpr int warps = (sizeof(T) == 8) ? (K == 1 ? 16 : 24) : 24;
     static constexpr int v = (warps / TY) > 0 ? (warps / TY) : 1;
 };
 
@@ -75,7 +76,7 @@ __device__ __forceinline__ int add3(int a, int k) { int t = a + k; return t >= 3
 
 // One 32 x TY x zchunk tile (tile coordinates bx, by, bz) of one domain.
 // Ends with a CTA-wide barrier, so the caller may reuse the shared memory.
-template <typename T, int TY, bool HEAT, bool DPPW, bool SOL>
+template <typename T, int TY, bool HEAT, bool DPPW, bool SOL, bool SMOOTH>
 __device__ __forceinline__ void fused_tile(const DomainDesc& d, const KC<T>& c, const T* __restrict__ phi_in,
                                            const T* __restrict__ c_in, T* __restrict__ phi_out,
                                            T* __restrict__ dpp, T* __restrict__ c_out,
@@ -278,8 +279,11 @@ __device__ __forceinline__ void fused_tile(const DomainDesc& d, const KC<T>& c, 
             if constexpr (ran_mode == 2) {
                 ran = (float)dppv;   // drawn and stored by the first pass
             } else {
-                ran = (c.rt == 2) ? phase_ran(2, x + 1, y + 1, z + 1, c.it)
-                                  : __double2float_rn(ran64(hash63_mix(hin)));
+                if constexpr (SMOOTH)
+                    ran = (c.rt == 2) ? phase_ran(2, x + 1, y + 1, z + 1, c.it)
+                                      : __double2float_rn(ran64(hash63_mix(hin)));
+                else
+                    ran = __double2float_rn(ran64(hash63_mix(hin)));
                 if constexpr (ran_mode == 1) dpp[id] = (T)ran;
             }
             return phase_ppnew<T, true>(nb, E, W, N, S, Tt, B, cpp, ran, c);
@@ -373,23 +377,25 @@ __device__ __forceinline__ void fused_tile(const DomainDesc& d, const KC<T>& c, 
     __syncthreads();
 }
 
-// single domain: one CTA per tile
-template <typename T, int TY, bool HEAT, bool DPPW, bool SOL>
-__global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY, HEAT ? 0 : 1>::v))
+// single domain: one CTA per tile.  SMOOTH: the kernel may draw the smooth
+// noise (compiled only where the pass draws noise and the deck asks for it).
+template <typename T, int TY, bool HEAT, bool DPPW, bool SOL, bool SMOOTH>
+__global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY, SMOOTH ? 1 : 0>::v))
     k_fused(DomainDesc d, const KC<T> c, const T* __restrict__ phi_in, const T* __restrict__ c_in,
             T* __restrict__ phi_out, T* __restrict__ dpp, T* __restrict__ c_out, const T* __restrict__ T_old,
             T* __restrict__ T_new, int zchunk)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    fused_tile<T, TY, HEAT, DPPW, SOL>(d, c, phi_in, c_in, phi_out, dpp, c_out, T_old, T_new, zchunk, blockIdx.x,
-                                       blockIdx.y, blockIdx.z, smem_raw);
+    fused_tile<T, TY, HEAT, DPPW, SOL, SMOOTH>(d, c, phi_in, c_in, phi_out, dpp, c_out, T_old, T_new, zchunk,
+                                               blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
 }
 
 // many domains: a persistent grid walks the work list.  PASS 0 is the first
 // pass of a step (temperatura + sweep 1, or the whole step with one sweep),
-// PASS 1 the last (sweep 2 + solute).
-template <typename T, int TY, int PASS, bool ONE_SWEEP>
-__global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY, PASS == 0 ? 0 : 1>::v))
+// PASS 1 the last (sweep 2 + solute).  SMOOTH: some domain of the batch
+// draws the smooth noise (the first pass then selects per domain).
+template <typename T, int TY, int PASS, bool ONE_SWEEP, bool SMOOTH>
+__global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY, SMOOTH ? 1 : 0>::v))
     k_fused_batch(const BatchDomain* __restrict__ doms, const BatchStep* __restrict__ steps,
                   const BatchItem* __restrict__ items, const int* __restrict__ n_items, int zchunk)
 {
@@ -410,15 +416,15 @@ __global__ void __launch_bounds__(32 * TY, (FusedOcc<T, TY, PASS == 0 ? 0 : 1>::
         const KC<T>& kc = skc;
         if (PASS == 0) {
             if (ONE_SWEEP)
-                fused_tile<T, TY, true, true, true>(D.d, kc, (const T*)D.phi[q], (const T*)D.c[qc], (T*)D.phi[1 - q],
+                fused_tile<T, TY, true, true, true, SMOOTH>(D.d, kc, (const T*)D.phi[q], (const T*)D.c[qc], (T*)D.phi[1 - q],
                                                     (T*)D.dpp, (T*)D.c[1 - qc], (const T*)D.T[qt], (T*)D.T[1 - qt],
                                                     zchunk, it.bx, it.by, it.bz, smem_raw);
             else
-                fused_tile<T, TY, true, false, false>(D.d, kc, (const T*)D.phi[q], (const T*)D.c[qc],
+                fused_tile<T, TY, true, false, false, SMOOTH>(D.d, kc, (const T*)D.phi[q], (const T*)D.c[qc],
                                                       (T*)D.phi[1 - q], (T*)D.dpp, nullptr, (const T*)D.T[qt],
                                                       (T*)D.T[1 - qt], zchunk, it.bx, it.by, it.bz, smem_raw);
         } else {
-            fused_tile<T, TY, false, true, true>(D.d, kc, (const T*)D.phi[1 - q], (const T*)D.c[qc], (T*)D.phi[q],
+            fused_tile<T, TY, false, true, true, false>(D.d, kc, (const T*)D.phi[1 - q], (const T*)D.c[qc], (T*)D.phi[q],
                                                  (T*)D.dpp, (T*)D.c[1 - qc], nullptr, nullptr, zchunk, it.bx, it.by,
                                                  it.bz, smem_raw);
         }
@@ -431,12 +437,12 @@ constexpr size_t fused_smem_bytes()
     return sizeof(FusedSmem<T, TY>);
 }
 
-template <typename T, int TY, bool HEAT, bool DPPW, bool SOL>
+template <typename T, int TY, bool HEAT, bool DPPW, bool SOL, bool SMOOTH>
 cudaError_t launch_fused_t(const DomainDesc& d, const StepArgs& s, const void* phi_in, const void* c_in,
                            void* phi_out, void* dpp, void* c_out, const void* T_old, void* T_new, int zchunk,
                            cudaStream_t st)
 {
-    auto kern = k_fused<T, TY, HEAT, DPPW, SOL>;
+    auto kern = k_fused<T, TY, HEAT, DPPW, SOL, SMOOTH>;
     const size_t smem = fused_smem_bytes<T, TY>();
     static bool configured = false;   // one attribute call per instantiation
     if (!configured) {
@@ -453,16 +459,19 @@ cudaError_t launch_fused_t(const DomainDesc& d, const StepArgs& s, const void* p
     return cudaGetLastError();
 }
 
-template <typename T, bool HEAT, bool DPPW, bool SOL>
+template <typename T, bool HEAT, bool DPPW, bool SOL, bool SMOOTH>
 cudaError_t launch_fused_ty(const DomainDesc& d, const StepArgs& s, const void* phi_in, const void* c_in,
                             void* phi_out, void* dpp, void* c_out, const void* T_old, void* T_new, int tile_y,
                             int zchunk, cudaStream_t st)
 {
+#define PF3D_TY_CASE(TYV) \
+    launch_fused_t<T, TYV, HEAT, DPPW, SOL, SMOOTH>(d, s, phi_in, c_in, phi_out, dpp, c_out, T_old, T_new, zchunk, st)
     switch (tile_y) {
-    case 4: return launch_fused_t<T, 4, HEAT, DPPW, SOL>(d, s, phi_in, c_in, phi_out, dpp, c_out, T_old, T_new, zchunk, st);
-    case 16: return launch_fused_t<T, 16, HEAT, DPPW, SOL>(d, s, phi_in, c_in, phi_out, dpp, c_out, T_old, T_new, zchunk, st);
-    default: return launch_fused_t<T, 8, HEAT, DPPW, SOL>(d, s, phi_in, c_in, phi_out, dpp, c_out, T_old, T_new, zchunk, st);
+    case 4: return PF3D_TY_CASE(4);
+    case 16: return PF3D_TY_CASE(16);
+    default: return PF3D_TY_CASE(8);
     }
+#undef PF3D_TY_CASE
 }
 
 // first pass of a step: temperatura + sweep 1 (phi_old -> phi_mid); with a
@@ -471,11 +480,16 @@ template <typename T>
 cudaError_t launch_fused_first(const DomainDesc& d, const StepArgs& s, const Fields& f, bool with_solute, int tile_y,
                                int zchunk, cudaStream_t st)
 {
+    const bool smooth = d.rt == 2;
     if (with_solute)
-        return launch_fused_ty<T, true, true, true>(d, s, f.phi_old, f.c_old, f.phi_mid, f.dpp, f.c_new, f.T_old,
-                                                    f.T_new, tile_y, zchunk, st);
-    return launch_fused_ty<T, true, false, false>(d, s, f.phi_old, f.c_old, f.phi_mid, f.dpp, nullptr, f.T_old, f.T_new,
-                                                  tile_y, zchunk, st);
+        return smooth ? launch_fused_ty<T, true, true, true, true>(d, s, f.phi_old, f.c_old, f.phi_mid, f.dpp, f.c_new,
+                                                                   f.T_old, f.T_new, tile_y, zchunk, st)
+                      : launch_fused_ty<T, true, true, true, false>(d, s, f.phi_old, f.c_old, f.phi_mid, f.dpp,
+                                                                    f.c_new, f.T_old, f.T_new, tile_y, zchunk, st);
+    return smooth ? launch_fused_ty<T, true, false, false, true>(d, s, f.phi_old, f.c_old, f.phi_mid, f.dpp, nullptr,
+                                                                 f.T_old, f.T_new, tile_y, zchunk, st)
+                  : launch_fused_ty<T, true, false, false, false>(d, s, f.phi_old, f.c_old, f.phi_mid, f.dpp, nullptr,
+                                                                  f.T_old, f.T_new, tile_y, zchunk, st);
 }
 
 // last pass: final sweep (phi_mid -> phi_new) with DPP + solute from phi_mid.
@@ -483,17 +497,17 @@ template <typename T>
 cudaError_t launch_fused_last(const DomainDesc& d, const StepArgs& s, const Fields& f, int tile_y, int zchunk,
                               cudaStream_t st)
 {
-    return launch_fused_ty<T, false, true, true>(d, s, f.phi_mid, f.c_old, f.phi_new, f.dpp, f.c_new, nullptr, nullptr,
-                                                 tile_y, zchunk, st);
+    return launch_fused_ty<T, false, true, true, false>(d, s, f.phi_mid, f.c_old, f.phi_new, f.dpp, f.c_new, nullptr,
+                                                        nullptr, tile_y, zchunk, st);
 }
 
 // The persistent grid is the SM count times the CTAs of this kernel that are
 // resident on one SM (each pass has its own register budget).
-template <typename T, int TY, int PASS, bool ONE_SWEEP>
+template <typename T, int TY, int PASS, bool ONE_SWEEP, bool SMOOTH>
 cudaError_t launch_batch_t(const BatchDomain* doms, const BatchStep* steps, const BatchItem* items, const int* n_items,
                            int zchunk, int n_sm, cudaStream_t st)
 {
-    auto kern = k_fused_batch<T, TY, PASS, ONE_SWEEP>;
+    auto kern = k_fused_batch<T, TY, PASS, ONE_SWEEP, SMOOTH>;
     const size_t smem = fused_smem_bytes<T, TY>();
     static int per_sm = 0;   // one attribute and occupancy query per instantiation
     if (per_sm == 0) {
@@ -510,20 +524,26 @@ cudaError_t launch_batch_t(const BatchDomain* doms, const BatchStep* steps, cons
 
 template <typename T>
 cudaError_t launch_fused_batch(const BatchDomain* doms, const BatchStep* steps, const BatchItem* items,
-                               const int* n_items, int pass, bool one_sweep, int tile_y, int zchunk, int n_sm,
-                               cudaStream_t st)
+                               const int* n_items, int pass, bool one_sweep, bool smooth, int tile_y, int zchunk,
+                               int n_sm, cudaStream_t st)
 {
-#define PF3D_BATCH_CASE(TYV)                                                                                   \
-    if (tile_y == TYV) {                                                                                       \
-        if (pass == 0)                                                                                         \
-            return one_sweep ? launch_batch_t<T, TYV, 0, true>(doms, steps, items, n_items, zchunk, n_sm, st)  \
-                             : launch_batch_t<T, TYV, 0, false>(doms, steps, items, n_items, zchunk, n_sm, st); \
-        return launch_batch_t<T, TYV, 1, false>(doms, steps, items, n_items, zchunk, n_sm, st);               \
+#define PF3D_BATCH_ARGS doms, steps, items, n_items, zchunk, n_sm, st
+#define PF3D_BATCH_CASE(TYV)                                                                          \
+    if (tile_y == TYV) {                                                                              \
+        if (pass == 0) {                                                                              \
+            if (one_sweep)                                                                            \
+                return smooth ? launch_batch_t<T, TYV, 0, true, true>(PF3D_BATCH_ARGS)                \
+                              : launch_batch_t<T, TYV, 0, true, false>(PF3D_BATCH_ARGS);              \
+            return smooth ? launch_batch_t<T, TYV, 0, false, true>(PF3D_BATCH_ARGS)                   \
+                          : launch_batch_t<T, TYV, 0, false, false>(PF3D_BATCH_ARGS);                 \
+        }                                                                                             \
+        return launch_batch_t<T, TYV, 1, false, false>(PF3D_BATCH_ARGS);                              \
     }
     PF3D_BATCH_CASE(4)
     PF3D_BATCH_CASE(16)
     PF3D_BATCH_CASE(8)
 #undef PF3D_BATCH_CASE
+#undef PF3D_BATCH_ARGS
     return cudaErrorInvalidValue;
 }
 

@@ -61,8 +61,8 @@ struct BatchItem {
 };
 template <typename T> cudaError_t launch_fused_batch(const BatchDomain* doms, const BatchStep* steps,
                                                      const BatchItem* items, const int* n_items, int pass,
-                                                     bool one_sweep, int tile_y, int zchunk, int n_sm,
-                                                     cudaStream_t st);
+                                                     bool one_sweep, bool smooth, int tile_y, int zchunk,
+                                                     int n_sm, cudaStream_t st);
 
 // Diagnostics: block partials into part[nblk*8], final into out[5].
 template <typename T> cudaError_t launch_diag(const DomainDesc& d, const void* phi, const void* c, double* part,

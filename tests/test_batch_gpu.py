@@ -50,6 +50,34 @@ def test_batch_equals_alone(gpu, prec):
                 assert np.array_equal(got[k], want[k]), (s, k)
 
 
+@pytest.mark.parametrize("prec", [pf3d.PF_FP64, pf3d.PF_FP32])
+def test_batch_mixed_noise_kinds(gpu, prec):
+    """A batch whose domains draw different noise (the smooth noise selects the
+    kernels that carry it) still gives each domain its alone result, before and
+    after the smooth-noise domain leaves."""
+    cases = [case(36, 20, 30), case(24, 40, 26, ruido_tipo=2, AAA=0.02), case(30, 30, 24, ruido_tipo=1)]
+    with pf3d.Batch(prec) as b:
+        slots = []
+        for g, p, st in cases:
+            s = b.add(g, p)
+            b.load_state(s, st)
+            slots.append(s)
+        b.step(4)
+        g, p, st = cases[1]
+        want, _ = alone(g, p, st, prec, 4)
+        got = b.fields(slots[1])
+        for k in want:
+            assert np.array_equal(got[k], want[k]), ("smooth", k)
+        b.remove(slots[1])
+        b.step(5)
+        for i in (0, 2):
+            g, p, st = cases[i]
+            want, _ = alone(g, p, st, prec, 9)
+            got = b.fields(slots[i])
+            for k in want:
+                assert np.array_equal(got[k], want[k]), (i, k)
+
+
 def test_batch_budget_and_membership(gpu):
     g, p, st = case(32, 32, 32)
     per = pf3d._abi.LIB.pf_ctx_bytes(pf3d._abi.C.byref(g), 32)
