@@ -37,10 +37,13 @@ UNIT = "GCell-updates/s"
 # algorithmic HBM bytes per cell and step of the fused step: phi, c, T, DPP
 # each read once and written once (8 B FP64 / 4 B FP32)
 STEP_BYTES_PER_CELL = {64: 64, 32: 32}
-# algorithmic bytes per cell of each fused pass:
-#   first = temperatura + sweep 1: reads phi, c, DPP; writes T, phi_mid
-#   last  = sweep 2 + solute     : reads phi_mid, c; writes phi, DPP, c
-PASS_BYTES_PER_CELL = {64: 40, 32: 20}
+# the step's algorithmic bytes split between the two fused passes, each state
+# byte counted in the pass that must move it:
+#   first = temperatura + sweep 1: reads phi, c, T, DPP; writes T   (5 fields)
+#   last  = sweep 2 + solute     : writes phi, DPP, c               (3 fields)
+# The passes also move phi_mid, the noise hand-over and a second read of c
+# (104 B/cell in FP64 by design); ncu's per-launch DRAM bytes are "traffic".
+PASS_BYTES_PER_CELL = {"fused_first": {64: 40, 32: 20}, "fused_last": {64: 24, 32: 12}}
 CPU_SAMPLE = (512, 512, 32)   # bounded CPU sample: bottom slab of the workload
 
 
@@ -52,6 +55,10 @@ def measured_peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def step_hbm_frac_of(gbs: float, peak: float) -> float:
+    return gbs / peak
 
 
 def ncu_traffic(kernel: str, precision: int):
@@ -136,6 +143,13 @@ def cpu_oracle_rate(precision_unused: int, seconds: float, warmup: int = 1, min_
     return (nx * ny * nz * n / dt / 1e9, n, dt, pyoracle.num_threads())
 
 
+def workload_config(w, p, world: int) -> dict:
+    es = 8 if w.precision == 64 else 4
+    return {"workload": w.name, "grid": [w.nx, w.ny, w.nz], "cells": w.cells, "precision": f"fp{w.precision}",
+            "sweeps_per_step": p.n_varreduras, "parallelism": f"replicas{world}",
+            "l2": f"inputs larger than L2 (resident state of 4 fields x {es} B x {w.cells / 1e6:.0f}M cells)"}
+
+
 def run_reference(args, rank: int, world: int):
     if rank != 0:
         return 0
@@ -161,7 +175,7 @@ def run_reference(args, rank: int, world: int):
         "metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": w.name, "cells": w.cells, "sample_cells": nx * ny * nz},
+        "data": "synthetic", "config": dict(workload_config(w, p, world), sample_cells=nx * ny * nz),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "reference CPU OpenMP path as the C restatement in oracle/ (no Fortran compiler in the image)",
@@ -309,15 +323,20 @@ def main():
     dom.set_option(pf3d.PF_OPT_KTIMING, 0)
     peak, peak_kind = measured_peaks()
     kname, n_k, ms_k = ("fused_first", nf, mf) if mf >= ml else ("fused_last", nl, ml)
-    alg_bytes = PASS_BYTES_PER_CELL[prec] * cells
+    alg_bytes = PASS_BYTES_PER_CELL[kname][prec] * cells
     avg_s = ms_k / max(1, n_k) / 1e3
     achieved = alg_bytes / avg_s / 1e9
     tr = ncu_traffic(kname, prec)
+    step_gbs = value / world * STEP_BYTES_PER_CELL[prec]
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": (tr * cells if tr is not None else None), "kernel": kname,
                 "kernel_ms": avg_s * 1e3, "peak_source": f"{peak_kind} hbm_gbs",
-                "shares": {"fused_first": mf / max(1e-9, mf + ml), "fused_last": ml / max(1e-9, mf + ml)}}
-    step_hbm_frac = value / world * STEP_BYTES_PER_CELL[prec] / peak
+                "alg_bytes_per_cell": PASS_BYTES_PER_CELL[kname][prec], "traffic_bytes_per_cell": tr,
+                "shares": {"fused_first": mf / max(1e-9, mf + ml), "fused_last": ml / max(1e-9, mf + ml)},
+                "step": {"achieved": step_gbs, "frac": step_hbm_frac_of(step_gbs, peak),
+                         "alg_bytes_per_cell": STEP_BYTES_PER_CELL[prec]},
+                "limiter": "instruction issue, not HBM (ncu: 69-78 % issue active, DRAM 8-22 % of peak)"}
+    step_hbm_frac = step_gbs / peak
 
     # ---- end to end through the C-ABI with pinned host buffers ----
     e2e = None
@@ -381,9 +400,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if prec == 64 else "f32", "data": "synthetic",
-        "config": {"workload": w.name, "grid": [w.nx, w.ny, w.nz], "cells": cells, "precision": f"fp{prec}",
-                   "sweeps_per_step": p.n_varreduras, "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (resident state of 4 fields x 8 B x 268M cells)"},
+        "config": workload_config(w, p, world),
         "hbm_frac_step": step_hbm_frac,
         "roofline": roofline,
         "cpu_baseline": cpu,
