@@ -211,6 +211,44 @@ int pf_diagnosticos_noalloc(const void* phase_field, const void* conc_soluto, in
    c = C0 (1 - (1 - Ke) phi); T = T0; DPP = 0.  At most 4096 bumps.        */
 int pf_init_seeded(pf_ctx* ctx, int n_bumps, const double* sites);
 
+/* ---- tracking, checkpoints, moving frame ------------------------------ */
+/* Solidification tracking on the device, no field copied to the host:
+   out = {solid fraction mean(phi >= 0.5), tip position, solid cells} of
+   phase_field_old (the state after the last step).  Tip position = the
+   highest 1-based plane k where some (i, j) column has phi >= 0.5, plus the
+   linear interpolation to the 0.5 crossing between the maxima of planes k
+   and k+1 (k itself when k = nz; 0 with no solid): the tip height of the
+   reference's run log (docs/run6/README.md:54-62) as karma/karma3d.f90:
+   291-298 tracks it.  Equal bit for bit to the same metric on the
+   downloaded field.                                                        */
+int pf_track(pf_ctx* ctx, double out[3]);
+
+/* Binary checkpoint of the domain's state (phase_field_old, conc_soluto_old,
+   TOLD, DPP in the context's precision, plus pf_state): no counterpart in
+   the reference, whose only restart is its 8-digit Tecplot text
+   (saida.f90:20-54 read back by entrada.f90:284-321).  A run continued from
+   a checkpoint gives the same bits as the run never stopped.
+   pf_checkpoint_save is asynchronous: it enqueues the device-to-host copy on
+   the context's stream and returns; a host thread writes the file once the
+   copy has landed, while the caller keeps stepping.  pf_checkpoint_wait
+   waits for that writer and returns its status; a second save, a load and
+   pf_destroy wait for it too.  pf_checkpoint_load is synchronous; the
+   file's grid and precision must be the context's.                        */
+int pf_checkpoint_save(pf_ctx* ctx, const char* path);
+int pf_checkpoint_wait(pf_ctx* ctx);
+int pf_checkpoint_load(pf_ctx* ctx, const char* path);
+
+/* Moving frame on the device, replacing the reference's manual restart with
+   a shift (entrada.f90:284-321, tipo_inicial = 4 with k_desl = R_semente):
+   phase_field_old and conc_soluto_old move down by k_desl planes (plane k
+   takes plane k + k_desl); the k_desl top planes become liquid, phi = 0 with
+   each column's c of the former top plane; conc_soluto_new = conc_soluto_old,
+   phase_field_new = 0, TOLD = TNEW = T0 and DPP = 0 (entrada's initial fill,
+   entrada.f90:239-262).  The pf_state is left alone (the reference's restart
+   starts a new run: set it with pf_set_state).  0 <= k_desl < nz, else
+   PF_E_ARG (entrada.f90:292).                                             */
+int pf_shift_frame(pf_ctx* ctx, int k_desl);
+
 /* ---- fused step ------------------------------------------------------- */
 /* Runs n_steps whole iterations of principal.f90:93-226 (temperatura, TP
    ramp, n_varreduras sweeps, solute, auxiliar, swap) with the fused
@@ -254,6 +292,13 @@ int pf_batch_set_tile(pf_batch* b, int tile_y, int zchunk);
    and caches it per shape class (precision, median column size and depth) */
 int pf_batch_autotune(pf_batch* b, int steps_per_candidate, int* tile_y, int* zchunk, double* ms_per_step);
 int pf_batch_diagnosticos(pf_batch* b, int slot, double out[5]);
+/* pf_track of one slot                                                    */
+int pf_batch_track(pf_batch* b, int slot, double out[3]);
+/* Checkpoint of one slot in pf_checkpoint_save's format (synchronous, so a
+   server may remove the slot right after it, e.g. to preempt the request);
+   load restores a slot added with the same grid, deck and precision.      */
+int pf_batch_checkpoint_save(pf_batch* b, int slot, const char* path);
+int pf_batch_checkpoint_load(pf_batch* b, int slot, const char* path);
 
 #ifdef __cplusplus
 }

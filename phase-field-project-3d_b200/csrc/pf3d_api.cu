@@ -11,12 +11,14 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 #include "../../include/pf3d.h"
 #include "pf3d_launch.h"
 #include "pf3d_scalar.h"
 #include "pf3d_hostdesc.h"
 #include "pf3d_init.cuh"
+#include "pf3d_ckpt.h"
 
 using namespace pf3d;
 
@@ -54,6 +56,16 @@ struct pf_ctx {
     double* h_out;     // pinned
     double* d_stage;
     size_t stage_elems;
+    unsigned long long* d_track;   // tracking scratch: nz plane maxima + count
+    double* d_track_out;           // 3 tracking results
+    // asynchronous checkpoint writer: fields copied into ckpt_host on the
+    // stream, then written to the file by ckpt_thr once ckpt_ev has passed
+    std::thread ckpt_thr;
+    void* ckpt_host;
+    size_t ckpt_host_bytes;
+    cudaEvent_t ckpt_ev;
+    int ckpt_rc;
+    std::string ckpt_err;
     cudaStream_t own_stream;
     cudaStream_t stream;
     int fused, tile_y, zchunk, ktiming;
@@ -135,7 +147,9 @@ int pf_create(const pf_grid* g, const pf_params* p, int precision, pf_ctx** out)
     // one allocation: 7 fields + diagnostics partials
     ctx->field_bytes = round_up((size_t)px * g->ny * g->nz * ctx->es + 64, 256);
     ctx->nblk = 592;
-    size_t total = 7 * ctx->field_bytes + (size_t)ctx->nblk * 8 * sizeof(double) + 8 * sizeof(double);
+    const size_t track_words = round_up((size_t)g->nz + 1, 4) + 4;
+    size_t total = 7 * ctx->field_bytes + (size_t)ctx->nblk * 8 * sizeof(double) + 8 * sizeof(double) +
+                   track_words * sizeof(unsigned long long);
     cudaError_t e = cudaMalloc(&ctx->base, total);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -145,6 +159,8 @@ int pf_create(const pf_grid* g, const pf_params* p, int precision, pf_ctx** out)
     for (int f = 0; f < 7; ++f) ctx->fld[f] = (char*)ctx->base + (size_t)f * ctx->field_bytes;
     ctx->d_part = (double*)((char*)ctx->base + 7 * ctx->field_bytes);
     ctx->d_out = ctx->d_part + (size_t)ctx->nblk * 8;
+    ctx->d_track = (unsigned long long*)(ctx->d_out + 8);
+    ctx->d_track_out = (double*)(ctx->d_track + round_up((size_t)g->nz + 1, 4));
     if ((e = cudaMemset(ctx->base, 0, total)) != cudaSuccess ||
         (e = cudaMallocHost(&ctx->h_out, 8 * sizeof(double))) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess) {
@@ -168,6 +184,9 @@ static void drop_events(pf_ctx* ctx)
 int pf_destroy(pf_ctx* ctx)
 {
     if (!ctx) return PF_OK;
+    if (ctx->ckpt_thr.joinable()) ctx->ckpt_thr.join();
+    if (ctx->ckpt_host) cudaFreeHost(ctx->ckpt_host);
+    if (ctx->ckpt_ev) cudaEventDestroy(ctx->ckpt_ev);
     cudaStreamSynchronize(ctx->stream);
     drop_events(ctx);
     if (ctx->d_stage) cudaFree(ctx->d_stage);
@@ -408,6 +427,132 @@ int pf_diagnosticos(pf_ctx* ctx, double out[5])
 {
     if (!ctx || !out) return PF_E_ARG;
     return run_diag(ctx, ctx->fld[PF_PHASE_NEW], ctx->fld[PF_CONC_NEW], out);
+}
+
+int pf_track(pf_ctx* ctx, double out[3])
+{
+    if (!ctx || !out) return PF_E_ARG;
+    CK(is64(ctx) ? launch_track<double>(ctx->dd, ctx->fld[PF_PHASE_OLD], ctx->d_track, ctx->d_track_out, ctx->stream)
+                 : launch_track<float>(ctx->dd, ctx->fld[PF_PHASE_OLD], ctx->d_track, ctx->d_track_out, ctx->stream),
+       "pf_track");
+    CK(cudaMemcpyAsync(ctx->h_out, ctx->d_track_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
+       "track copy");
+    CK(cudaStreamSynchronize(ctx->stream), "track sync");
+    std::memcpy(out, ctx->h_out, 3 * sizeof(double));
+    return PF_OK;
+}
+
+// ---- checkpoints ----
+
+int pf_checkpoint_wait(pf_ctx* ctx)
+{
+    if (!ctx) return PF_E_ARG;
+    if (ctx->ckpt_thr.joinable()) ctx->ckpt_thr.join();
+    const int rc = ctx->ckpt_rc;
+    ctx->ckpt_rc = PF_OK;
+    if (rc != PF_OK) return ctx_err(ctx, rc, "pf_checkpoint_save: " + ctx->ckpt_err);
+    return PF_OK;
+}
+
+static int ckpt_host_buffer(pf_ctx* ctx, size_t bytes)
+{
+    if (ctx->ckpt_host_bytes >= bytes) return PF_OK;
+    if (ctx->ckpt_host) cudaFreeHost(ctx->ckpt_host);
+    ctx->ckpt_host = nullptr;
+    ctx->ckpt_host_bytes = 0;
+    CK(cudaMallocHost(&ctx->ckpt_host, bytes), "checkpoint host buffer");
+    ctx->ckpt_host_bytes = bytes;
+    return PF_OK;
+}
+
+int pf_checkpoint_save(pf_ctx* ctx, const char* path)
+{
+    if (!ctx || !path) return PF_E_ARG;
+    int rc = pf_checkpoint_wait(ctx);   // one writer at a time
+    if (rc != PF_OK) return rc;
+    const pf_grid& g = ctx->g;
+    const size_t row = (size_t)g.nx * ctx->es;
+    const size_t fbytes = row * g.ny * g.nz;
+    if ((rc = ckpt_host_buffer(ctx, 4 * fbytes)) != PF_OK) return rc;
+    if (!ctx->ckpt_ev) CK(cudaEventCreateWithFlags(&ctx->ckpt_ev, cudaEventDisableTiming), "checkpoint event");
+    for (int i = 0; i < 4; ++i)
+        CK(cudaMemcpy2DAsync((char*)ctx->ckpt_host + i * fbytes, row, ctx->fld[kCkptFields[i]],
+                             (size_t)ctx->dd.px * ctx->es, row, (size_t)g.ny * g.nz, cudaMemcpyDeviceToHost,
+                             ctx->stream),
+           "checkpoint copy");
+    CK(cudaEventRecord(ctx->ckpt_ev, ctx->stream), "checkpoint event");
+    // the host state of the copied fields: later steps are enqueued after them
+    const CkptHeader h = ckpt_header(g, ctx->prec, ctx->st);
+    const std::string file(path);
+    void* data = ctx->ckpt_host;
+    cudaEvent_t ev = ctx->ckpt_ev;
+    ctx->ckpt_thr = std::thread([ctx, h, file, data, fbytes, ev]() {
+        cudaError_t e = cudaEventSynchronize(ev);
+        if (e != cudaSuccess) {
+            ctx->ckpt_err = std::string("copy: ") + cudaGetErrorString(e);
+            ctx->ckpt_rc = PF_E_CUDA;
+            return;
+        }
+        std::string why = ckpt_write(file, h, data, fbytes);
+        if (!why.empty()) {
+            ctx->ckpt_err = why;
+            ctx->ckpt_rc = PF_E_STATE;
+        }
+    });
+    return PF_OK;
+}
+
+int pf_checkpoint_load(pf_ctx* ctx, const char* path)
+{
+    if (!ctx || !path) return PF_E_ARG;
+    int rc = pf_checkpoint_wait(ctx);
+    if (rc != PF_OK) return rc;
+    std::FILE* f = std::fopen(path, "rb");
+    if (!f) return ctx_err(ctx, PF_E_ARG, std::string("pf_checkpoint_load: cannot open ") + path);
+    CkptHeader h;
+    std::string why = ckpt_read_header(f, ctx->g, ctx->prec, &h);
+    const pf_grid& g = ctx->g;
+    const size_t row = (size_t)g.nx * ctx->es;
+    const size_t fbytes = row * g.ny * g.nz;
+    if (why.empty() && ckpt_host_buffer(ctx, 4 * fbytes) != PF_OK) why = "cannot allocate the host buffer";
+    if (why.empty() && std::fread(ctx->ckpt_host, fbytes, 4, f) != 4) why = "checkpoint shorter than its fields";
+    std::fclose(f);
+    if (!why.empty()) return ctx_err(ctx, PF_E_ARG, "pf_checkpoint_load: " + why);
+    for (int i = 0; i < 4; ++i)
+        CK(cudaMemcpy2DAsync(ctx->fld[kCkptFields[i]], (size_t)ctx->dd.px * ctx->es,
+                             (const char*)ctx->ckpt_host + i * fbytes, row, row, (size_t)g.ny * g.nz,
+                             cudaMemcpyHostToDevice, ctx->stream),
+           "checkpoint upload");
+    CK(cudaStreamSynchronize(ctx->stream), "checkpoint sync");
+    ctx->st = ckpt_state(h);
+    return PF_OK;
+}
+
+// ---- moving frame ----
+
+int pf_shift_frame(pf_ctx* ctx, int k_desl)
+{
+    if (!ctx) return PF_E_ARG;
+    if (k_desl < 0 || k_desl >= ctx->g.nz)
+        return ctx_err(ctx, PF_E_ARG, "pf_shift_frame: the shift must be in [0, nz)");   // entrada.f90:292
+    const long long n = (long long)ctx->field_bytes / (long long)ctx->es;
+    void*& po = ctx->fld[PF_PHASE_OLD];
+    void*& pn = ctx->fld[PF_PHASE_NEW];
+    void*& co = ctx->fld[PF_CONC_OLD];
+    void*& cn = ctx->fld[PF_CONC_NEW];
+    CK(is64(ctx) ? launch_shift_frame<double>(ctx->dd, k_desl, po, co, pn, cn, ctx->stream)
+                 : launch_shift_frame<float>(ctx->dd, k_desl, po, co, pn, cn, ctx->stream),
+       "pf_shift_frame");
+    std::swap(po, pn);
+    std::swap(co, cn);
+    CK(cudaMemcpyAsync(cn, co, ctx->field_bytes, cudaMemcpyDeviceToDevice, ctx->stream), "shift: c_new");
+    CK(cudaMemsetAsync(pn, 0, ctx->field_bytes, ctx->stream), "shift: phi_new");
+    CK(cudaMemsetAsync(ctx->fld[PF_DPP], 0, ctx->field_bytes, ctx->stream), "shift: DPP");
+    for (int fidx : {PF_TOLD, PF_TNEW})
+        CK(is64(ctx) ? launch_fill<double>(ctx->fld[fidx], n, ctx->p.T0, ctx->stream)
+                     : launch_fill<float>(ctx->fld[fidx], n, ctx->p.T0, ctx->stream),
+           "shift: T");
+    return PF_OK;
 }
 
 int pf_swap(pf_ctx* ctx)

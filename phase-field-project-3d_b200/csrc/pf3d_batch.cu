@@ -26,6 +26,7 @@
 #include <vector>
 #include "../../include/pf3d.h"
 #include "pf3d_hostdesc.h"
+#include "pf3d_ckpt.h"
 #include "pf3d_init.cuh"
 
 using namespace pf3d;
@@ -74,6 +75,8 @@ struct pf_batch {
     int* d_nitems = nullptr;
     bool items_dirty = true;
     double* d_part = nullptr;          // diagnostics partials (592 x 8) + result
+    unsigned long long* d_track = nullptr;   // tracking scratch (grown to the tallest slot tracked)
+    int track_cap = 0;                 // planes it holds
     double* h_out = nullptr;
     double* d_sites = nullptr;         // bump sites for device initialisation
     int tile_y = 8, zchunk = 64, n_sm = 0;   // persistent grids: n_sm x resident CTAs
@@ -309,6 +312,7 @@ int pf_batch_destroy(pf_batch* b)
     cudaFree(b->d_items);
     cudaFree(b->d_nitems);
     cudaFree(b->d_part);
+    if (b->d_track) cudaFree(b->d_track);
     cudaFree(b->d_sites);
     cudaFreeHost(b->h_out);
     for (cudaEvent_t ev : {b->h_ev[0], b->h_ev[1], b->ev0, b->ev1})
@@ -623,6 +627,79 @@ int pf_batch_autotune(pf_batch* b, int steps_per_candidate, int* tile_y, int* zc
     if (zchunk) *zchunk = bzc;
     if (ms_per_step) *ms_per_step = best;
     return rc;
+}
+
+int pf_batch_track(pf_batch* b, int slot, double out[3])
+{
+    Slot* sl = get_slot(b, slot);
+    if (!sl || !out) return berr(b, PF_E_ARG, "pf_batch_track: bad argument");
+    const int nz = sl->g.nz;
+    if (nz > b->track_cap) {
+        BCK(cudaStreamSynchronize(b->stream), "track sync");
+        if (b->d_track) cudaFree(b->d_track);
+        b->d_track = nullptr;
+        b->track_cap = 0;
+        BCK(cudaMalloc(&b->d_track, ((size_t)nz + 1 + 4) * sizeof(unsigned long long)), "track scratch");
+        b->track_cap = nz;
+    }
+    double* res = (double*)(b->d_track + b->track_cap + 1);
+    cudaError_t e = b64(b) ? launch_track<double>(sl->bd.d, slot_field(*sl, PF_PHASE_OLD), b->d_track, res, b->stream)
+                           : launch_track<float>(sl->bd.d, slot_field(*sl, PF_PHASE_OLD), b->d_track, res, b->stream);
+    BCK(e, "pf_batch_track");
+    BCK(cudaMemcpyAsync(b->h_out, res, 3 * sizeof(double), cudaMemcpyDeviceToHost, b->stream), "track copy");
+    BCK(cudaStreamSynchronize(b->stream), "track sync");
+    std::memcpy(out, b->h_out, 3 * sizeof(double));
+    return PF_OK;
+}
+
+// A checkpoint of one slot, in the format of pf_checkpoint_save (synchronous:
+// the caller may remove the slot as soon as this returns).
+int pf_batch_checkpoint_save(pf_batch* b, int slot, const char* path)
+{
+    Slot* sl = get_slot(b, slot);
+    if (!sl || !path) return berr(b, PF_E_ARG, "pf_batch_checkpoint_save: bad argument");
+    const pf_grid& g = sl->g;
+    const size_t row = (size_t)g.nx * b->es;
+    const size_t fbytes = row * g.ny * g.nz;
+    std::vector<char> host(4 * fbytes);
+    for (int i = 0; i < 4; ++i)
+        BCK(cudaMemcpy2DAsync(host.data() + i * fbytes, row, slot_field(*sl, kCkptFields[i]),
+                              (size_t)sl->bd.d.px * b->es, row, (size_t)g.ny * g.nz, cudaMemcpyDeviceToHost,
+                              b->stream),
+            "checkpoint copy");
+    BCK(cudaStreamSynchronize(b->stream), "checkpoint sync");
+    const std::string why = ckpt_write(path, ckpt_header(g, b->prec, sl->st), host.data(), fbytes);
+    if (!why.empty()) return berr(b, PF_E_STATE, "pf_batch_checkpoint_save: " + why);
+    return PF_OK;
+}
+
+// Restores a slot (added with the same grid, deck and precision) from a
+// checkpoint; the slot continues from the checkpoint's step.
+int pf_batch_checkpoint_load(pf_batch* b, int slot, const char* path)
+{
+    Slot* sl = get_slot(b, slot);
+    if (!sl || !path) return berr(b, PF_E_ARG, "pf_batch_checkpoint_load: bad argument");
+    std::FILE* f = std::fopen(path, "rb");
+    if (!f) return berr(b, PF_E_ARG, std::string("pf_batch_checkpoint_load: cannot open ") + path);
+    const pf_grid& g = sl->g;
+    CkptHeader h;
+    std::string why = ckpt_read_header(f, g, b->prec, &h);
+    const size_t row = (size_t)g.nx * b->es;
+    const size_t fbytes = row * g.ny * g.nz;
+    std::vector<char> host;
+    if (why.empty()) {
+        host.resize(4 * fbytes);
+        if (std::fread(host.data(), fbytes, 4, f) != 4) why = "checkpoint shorter than its fields";
+    }
+    std::fclose(f);
+    if (!why.empty()) return berr(b, PF_E_ARG, "pf_batch_checkpoint_load: " + why);
+    for (int i = 0; i < 4; ++i)
+        BCK(cudaMemcpy2DAsync(slot_field(*sl, kCkptFields[i]), (size_t)sl->bd.d.px * b->es, host.data() + i * fbytes,
+                              row, row, (size_t)g.ny * g.nz, cudaMemcpyHostToDevice, b->stream),
+            "checkpoint upload");
+    BCK(cudaStreamSynchronize(b->stream), "checkpoint sync");
+    sl->st = ckpt_state(h);
+    return PF_OK;
 }
 
 int pf_batch_diagnosticos(pf_batch* b, int slot, double out[5])

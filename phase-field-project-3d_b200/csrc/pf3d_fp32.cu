@@ -2,6 +2,8 @@
 // diagnostics still accumulate in FP64).
 #include "pf3d_simple.cuh"
 #include "pf3d_init.cuh"
+#include "pf3d_track.cuh"
+#include "pf3d_frame.cuh"
 #include "pf3d_fused.cuh"
 
 namespace pf3d {
@@ -20,5 +22,22 @@ cudaError_t launch_init_seeded<float>(const DomainDesc& d, const InitArgs& a, co
                                   void* Tf, void* dpp, cudaStream_t st)
 {
     return launch_init_seeded_impl<float>(d, a, sites, phi, c, Tf, dpp, st);
+}
+template <>
+cudaError_t launch_track<float>(const DomainDesc& d, const void* phi, unsigned long long* scratch, double* out,
+                             cudaStream_t st)
+{
+    return launch_track_impl<float>(d, phi, scratch, out, st);
+}
+template <>
+cudaError_t launch_shift_frame<float>(const DomainDesc& d, int kd, const void* phi_o, const void* c_o, void* phi_n,
+                                   void* c_n, cudaStream_t st)
+{
+    return launch_shift_frame_impl<float>(d, kd, phi_o, c_o, phi_n, c_n, st);
+}
+template <>
+cudaError_t launch_fill<float>(void* a, long long n, double v, cudaStream_t st)
+{
+    return launch_fill_impl<float>(a, n, v, st);
 }
 }  // namespace pf3d

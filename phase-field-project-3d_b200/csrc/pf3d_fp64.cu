@@ -4,6 +4,8 @@
 // no fused multiply-add, so neither may this form.
 #include "pf3d_simple.cuh"
 #include "pf3d_init.cuh"
+#include "pf3d_track.cuh"
+#include "pf3d_frame.cuh"
 
 namespace pf3d {
 template cudaError_t launch_heat<double>(const DomainDesc&, const StepArgs&, const Fields&, cudaStream_t);
@@ -18,5 +20,22 @@ cudaError_t launch_init_seeded<double>(const DomainDesc& d, const InitArgs& a, c
                                   void* Tf, void* dpp, cudaStream_t st)
 {
     return launch_init_seeded_impl<double>(d, a, sites, phi, c, Tf, dpp, st);
+}
+template <>
+cudaError_t launch_track<double>(const DomainDesc& d, const void* phi, unsigned long long* scratch, double* out,
+                             cudaStream_t st)
+{
+    return launch_track_impl<double>(d, phi, scratch, out, st);
+}
+template <>
+cudaError_t launch_shift_frame<double>(const DomainDesc& d, int kd, const void* phi_o, const void* c_o, void* phi_n,
+                                   void* c_n, cudaStream_t st)
+{
+    return launch_shift_frame_impl<double>(d, kd, phi_o, c_o, phi_n, c_n, st);
+}
+template <>
+cudaError_t launch_fill<double>(void* a, long long n, double v, cudaStream_t st)
+{
+    return launch_fill_impl<double>(a, n, v, st);
 }
 }  // namespace pf3d

@@ -64,6 +64,17 @@ template <typename T> cudaError_t launch_fused_batch(const BatchDomain* doms, co
                                                      bool one_sweep, bool smooth, int tile_y, int zchunk,
                                                      int n_sm, cudaStream_t st);
 
+// Solidification tracking of phi: out[3] = {solid fraction, tip position
+// (cells, 1-based), solid cells}; scratch holds nz + 1 words.
+template <typename T> cudaError_t launch_track(const DomainDesc& d, const void* phi, unsigned long long* scratch,
+                                               double* out, cudaStream_t st);
+
+// Moving frame (restart with a shift of kd planes) into the "new" buffers;
+// fill of n elements with v.
+template <typename T> cudaError_t launch_shift_frame(const DomainDesc& d, int kd, const void* phi_o, const void* c_o,
+                                                     void* phi_n, void* c_n, cudaStream_t st);
+template <typename T> cudaError_t launch_fill(void* a, long long n, double v, cudaStream_t st);
+
 // Diagnostics: block partials into part[nblk*8], final into out[5].
 template <typename T> cudaError_t launch_diag(const DomainDesc& d, const void* phi, const void* c, double* part,
                                               int nblk, double* out, cudaStream_t st);

@@ -11,6 +11,7 @@ the C-ABI of libpf3d.so; nothing here computes on the CPU.
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -195,6 +196,31 @@ class Domain:
         self._chk(LIB.pf_step_diag(self._h, int(n), out))
         return tuple(out)
 
+    # ---- tracking, checkpoints, moving frame ----
+    def track(self):
+        """(solid fraction, tip position in cells, solid cells) of the current
+        phase field, evaluated on the device (pf_track)."""
+        out = (C.c_double * 3)()
+        self._chk(LIB.pf_track(self._h, out))
+        return out[0], out[1], int(out[2])
+
+    def checkpoint(self, path: str, wait: bool = False):
+        """Binary checkpoint of the state; the file is written by a host
+        thread while the domain keeps stepping (pf_checkpoint_save)."""
+        self._chk(LIB.pf_checkpoint_save(self._h, os.fsencode(path)))
+        if wait:
+            self.checkpoint_wait()
+
+    def checkpoint_wait(self):
+        self._chk(LIB.pf_checkpoint_wait(self._h))
+
+    def restore(self, path: str):
+        self._chk(LIB.pf_checkpoint_load(self._h, os.fsencode(path)))
+
+    def shift_frame(self, k_desl: int):
+        """The reference's restart with a shift of k_desl planes, on the device."""
+        self._chk(LIB.pf_shift_frame(self._h, int(k_desl)))
+
     def kernel_times(self, reset: bool = True):
         nf, nl = C.c_long(), C.c_long()
         mf, ml = C.c_double(), C.c_double()
@@ -314,6 +340,17 @@ class Batch:
         out = (C.c_double * 5)()
         self._chk(LIB.pf_batch_diagnosticos(self._h, slot, out))
         return tuple(out)
+
+    def track(self, slot: int):
+        out = (C.c_double * 3)()
+        self._chk(LIB.pf_batch_track(self._h, slot, out))
+        return out[0], out[1], int(out[2])
+
+    def checkpoint(self, slot: int, path: str):
+        self._chk(LIB.pf_batch_checkpoint_save(self._h, slot, os.fsencode(path)))
+
+    def restore(self, slot: int, path: str):
+        self._chk(LIB.pf_batch_checkpoint_load(self._h, slot, os.fsencode(path)))
 
     def fields(self, slot: int) -> dict:
         return {"phi": self.download(slot, PF_PHASE_OLD), "c": self.download(slot, PF_CONC_OLD),

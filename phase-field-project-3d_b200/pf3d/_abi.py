@@ -82,6 +82,11 @@ SIGNATURES = [
     ("pf_step", C.c_int, [_P, C.c_int]),
     ("pf_step_diag", C.c_int, [_P, C.c_int, _D]),
     ("pf_init_seeded", C.c_int, [_P, C.c_int, _D]),
+    ("pf_track", C.c_int, [_P, _D]),
+    ("pf_checkpoint_save", C.c_int, [_P, C.c_char_p]),
+    ("pf_checkpoint_wait", C.c_int, [_P]),
+    ("pf_checkpoint_load", C.c_int, [_P, C.c_char_p]),
+    ("pf_shift_frame", C.c_int, [_P, C.c_int]),
     ("pf_batch_create", C.c_int, [C.c_int, C.c_longlong, C.c_int, C.POINTER(_P)]),
     ("pf_batch_destroy", C.c_int, [_P]),
     ("pf_batch_set_stream", C.c_int, [_P, _P]),
@@ -99,6 +104,9 @@ SIGNATURES = [
     ("pf_batch_set_tile", C.c_int, [_P, C.c_int, C.c_int]),
     ("pf_batch_autotune", C.c_int, [_P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _D]),
     ("pf_batch_diagnosticos", C.c_int, [_P, C.c_int, _D]),
+    ("pf_batch_track", C.c_int, [_P, C.c_int, _D]),
+    ("pf_batch_checkpoint_save", C.c_int, [_P, C.c_int, C.c_char_p]),
+    ("pf_batch_checkpoint_load", C.c_int, [_P, C.c_int, C.c_char_p]),
     ("pf_diagnosticos_noalloc", C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                           C.c_double, C.c_double, C.c_double, C.c_double, _P, _D]),
 ]

@@ -14,8 +14,10 @@ with probability 0.2 and parameters drawn as in the batching configuration.
 admitted FIFO while they fit the device-memory budget (their state is
 created on the device), every admitted request advances together with the
 others in quanta of steps (one pf_batch_step per precision), and a request
-retires -- its diagnostics read back, its memory freed -- as soon as it has
-done its steps, which lets the next waiting requests in.  Latency of a
+retires -- its diagnostics and its solid fraction and tip position
+(evaluated on the device) read back, its memory freed -- as soon as it has
+done its steps, which lets the next waiting requests in.  No field ever
+leaves the device.  Latency of a
 request = completion time - arrival time.
 """
 from __future__ import annotations
@@ -52,7 +54,8 @@ class Job:
     admitted: float = -1.0
     done: float = -1.0
     slot: int = -1
-    result: tuple = ()
+    result: tuple = ()      # diagnostics of the final state (pf_batch_diagnosticos)
+    track: tuple = ()       # solid fraction, tip position, solid cells (pf_batch_track)
 
     @property
     def cells(self) -> int:
@@ -140,6 +143,7 @@ class Server:
             for slot, job in list(self.active[prec].items()):
                 if b.state(slot).it >= job.steps:
                     job.result = b.diagnosticos(slot)
+                    job.track = b.track(slot)
                     job.done = now
                     b.remove(slot)
                     self.used -= ctx_bytes(job)

@@ -148,4 +148,6 @@ def test_server_alone_vs_mix(gpu):
         with pf3d.Domain(j.grid(), j.params(), j.precision) as d:
             pf3d.init_seeded(d, j.sites())
             out = d.step_diag(j.steps)
+            tr = d.track()
         assert np.array_equal(np.array(out), np.array(j.result)), j.jid
+        assert tr == j.track, j.jid
