@@ -300,6 +300,60 @@ int pf_batch_track(pf_batch* b, int slot, double out[3]);
 int pf_batch_checkpoint_save(pf_batch* b, int slot, const char* path);
 int pf_batch_checkpoint_load(pf_batch* b, int slot, const char* path);
 
+/* ---- the quantitative Karma model (karma/karma3d.f90) ----------------- */
+/* The reference's second model: isothermal free growth of a dilute binary
+   alloy (Karma PRL 87 115701 2001; Echebarria, Folch, Karma & Plapp PRE 70
+   061604 2004) with phi in [-1, 1], the dimensionless supersaturation U,
+   cubic anisotropy eps4, the anti-trapping current and mirror (zero-flux)
+   faces, in units of the interface width W and time tau0.  The namelist of
+   karma.nml by its names (karma3d.f90:80-95); the reference's domain is
+   N^3 (nx = ny = nz = N), any extents are accepted here.                  */
+typedef struct pf_karma_params {
+    int    nx, ny, nz;
+    double lambda;         /* coupling constant, W/d0 = lambda/a1              */
+    double eps4;           /* cubic anisotropy of the interface energy         */
+    double dx;             /* cell size [W]                                    */
+    double dt;             /* time step [tau0]                                 */
+    double R0;             /* seed radius [W]                                  */
+    double Fnoise;         /* noise amplitude of the phase equation            */
+    double k, Tm, mliq, C0, TP, sigma, dH, Dl;   /* alloy (entrada.dat data)   */
+} pf_karma_params;
+
+/* dimensional scales of karma3d.f90:118-124                                */
+typedef struct pf_karma_derived {
+    double D;              /* a2 lambda (dimensionless diffusivity)           */
+    double cl0, Omega;     /* liquidus concentration at TP; supersaturation   */
+    double Gam, d0;        /* Gibbs-Thomson coefficient; capillary length [m] */
+    double W, tau0;        /* interface width [m]; relaxation time [s]        */
+} pf_karma_derived;
+
+#define PF_KARMA_PHI  0
+#define PF_KARMA_U    1
+#define PF_KARMA_DPHI 2    /* dphi/dt of the last step (download only)       */
+
+typedef struct pf_karma pf_karma;
+int pf_karma_derived_of(const pf_karma_params* p, pf_karma_derived* out);
+int pf_karma_create(const pf_karma_params* p, int precision, pf_karma** out);
+int pf_karma_destroy(pf_karma* k);
+int pf_karma_set_stream(pf_karma* k, void* stream);
+/* steps done (the noise of step n uses it = n, karma3d.f90:161)            */
+int pf_karma_get_it(const pf_karma* k, int* it);
+int pf_karma_set_it(pf_karma* k, int it);
+/* interior cells, Fortran order (nx*ny*nz doubles)                         */
+int pf_karma_upload(pf_karma* k, int field, const double* host);
+int pf_karma_download(pf_karma* k, int field, double* host);
+/* karma3d.f90:130-144 on the device: an eighth of a sphere of radius R0 at
+   the corner (phi = -tanh((r - R0)/sqrt 2)), U = -Omega; it = 0            */
+int pf_karma_seed(pf_karma* k);
+/* n_steps iterations of karma3d.f90:160-287 (mirror faces, phase equation,
+   U equation with the anti-trapping current, clamp and advance); in FP64
+   every operation is the reference's, in its order                       */
+int pf_karma_step(pf_karma* k, int n_steps);
+/* karma3d.f90:290-296: the largest i with phi(i,1,1) > 0 and with
+   phi(i,i,i) > 0 (1-based; 0 if none), evaluated on the device             */
+int pf_karma_tip(pf_karma* k, int* tip_x, int* tip_d);
+int pf_karma_sync(pf_karma* k);
+
 #ifdef __cplusplus
 }
 #endif

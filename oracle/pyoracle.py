@@ -162,3 +162,57 @@ class Oracle:
 
 def num_threads() -> int:
     return LIB.orc_num_threads()
+
+
+# ---- the quantitative Karma model (karma/karma3d.f90) ----
+LIB.orc_karma_ruido.restype = C.c_double
+LIB.orc_karma_ruido.argtypes = [C.c_int] * 4
+LIB.orc_karma_create.restype = _V
+LIB.orc_karma_create.argtypes = [C.c_int, C.c_int, C.c_int] + [C.c_double] * 6
+LIB.orc_karma_destroy.argtypes = [_V]
+LIB.orc_karma_set.argtypes = [_V, _V, _V]
+LIB.orc_karma_get.argtypes = [_V, _V, _V, _V]
+LIB.orc_karma_step.argtypes = [_V, C.c_int]
+LIB.orc_karma_set_it.argtypes = [_V, C.c_int]
+LIB.orc_karma_tip.argtypes = [_V, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+
+
+def karma_ruido(i, j, k, it) -> float:
+    return LIB.orc_karma_ruido(i, j, k, it)
+
+
+class KarmaOracle:
+    """karma3d.f90's time loop on the CPU (fields of shape (nz, ny, nx))."""
+
+    def __init__(self, nx, ny, nz, lambda_, eps4, dx, dt, Fnoise, k):
+        self.shape = (nz, ny, nx)
+        self._h = LIB.orc_karma_create(nx, ny, nz, lambda_, eps4, dx, dt, Fnoise, k)
+
+    def close(self):
+        if self._h:
+            LIB.orc_karma_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def set(self, phi: np.ndarray, U: np.ndarray):
+        a = np.ascontiguousarray(phi, dtype=np.float64)
+        b = np.ascontiguousarray(U, dtype=np.float64)
+        LIB.orc_karma_set(self._h, a.ctypes.data_as(_V), b.ctypes.data_as(_V))
+
+    def get(self):
+        phi, U, dphi = (np.empty(self.shape) for _ in range(3))
+        LIB.orc_karma_get(self._h, phi.ctypes.data_as(_V), U.ctypes.data_as(_V), dphi.ctypes.data_as(_V))
+        return phi, U, dphi
+
+    def step(self, n: int = 1):
+        LIB.orc_karma_step(self._h, n)
+
+    def set_it(self, it: int):
+        LIB.orc_karma_set_it(self._h, it)
+
+    def tip(self):
+        a, b = C.c_int(), C.c_int()
+        LIB.orc_karma_tip(self._h, C.byref(a), C.byref(b))
+        return a.value, b.value

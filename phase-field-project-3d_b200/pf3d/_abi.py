@@ -48,8 +48,21 @@ class pf_state(C.Structure):
                 ("Cs_eq", C.c_double), ("Cl_eq", C.c_double), ("time", C.c_float)]
 
 
+class pf_karma_params(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int)] + [
+        (n, C.c_double) for n in ("lambda_", "eps4", "dx", "dt", "R0", "Fnoise", "k", "Tm", "mliq", "C0", "TP",
+                                  "sigma", "dH", "Dl")]
+
+
+class pf_karma_derived(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("D", "cl0", "Omega", "Gam", "d0", "W", "tau0")]
+
+
+PF_KARMA_PHI, PF_KARMA_U, PF_KARMA_DPHI = 0, 1, 2
+
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
 
 # (name, restype, argtypes) for every function include/pf3d.h declares
 SIGNATURES = [
@@ -107,6 +120,18 @@ SIGNATURES = [
     ("pf_batch_track", C.c_int, [_P, C.c_int, _D]),
     ("pf_batch_checkpoint_save", C.c_int, [_P, C.c_int, C.c_char_p]),
     ("pf_batch_checkpoint_load", C.c_int, [_P, C.c_int, C.c_char_p]),
+    ("pf_karma_derived_of", C.c_int, [C.POINTER(pf_karma_params), C.POINTER(pf_karma_derived)]),
+    ("pf_karma_create", C.c_int, [C.POINTER(pf_karma_params), C.c_int, C.POINTER(_P)]),
+    ("pf_karma_destroy", C.c_int, [_P]),
+    ("pf_karma_set_stream", C.c_int, [_P, _P]),
+    ("pf_karma_get_it", C.c_int, [_P, _I]),
+    ("pf_karma_set_it", C.c_int, [_P, C.c_int]),
+    ("pf_karma_upload", C.c_int, [_P, C.c_int, _P]),
+    ("pf_karma_download", C.c_int, [_P, C.c_int, _P]),
+    ("pf_karma_seed", C.c_int, [_P]),
+    ("pf_karma_step", C.c_int, [_P, C.c_int]),
+    ("pf_karma_tip", C.c_int, [_P, _I, _I]),
+    ("pf_karma_sync", C.c_int, [_P]),
     ("pf_diagnosticos_noalloc", C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                           C.c_double, C.c_double, C.c_double, C.c_double, _P, _D]),
 ]
