@@ -228,6 +228,44 @@ def bench_batch(args, pf3d, serve, init):
             "tile": [32, ty, zc], "autotune_s": tune_s, "launch": "persistent work-list kernels, CUDA graph of 8 steps"}
 
 
+def bench_karma(args, torch, stream):
+    """The reference's second model (karma/karma3d.f90) on 512^3, FP64 and
+    FP32, seeded on the device, with a CPU-oracle sample for scale."""
+    from pf3d import karma
+    out = {"workload": "karma_512cube_Fnoise0.01", "unit": UNIT}
+    for prec in (64, 32):
+        p = karma.karma_params(N=512, Fnoise=0.01)
+        with karma.Karma(p, prec) as k:
+            k.set_stream(stream.cuda_stream)
+            k.seed()
+            k.step(args.warmup)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            n = max(10, args.steps // 2)
+            e0.record(stream)
+            k.step(n)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / n
+            out[f"fp{prec}"] = {"ms_per_step": ms, "value": 512 ** 3 / (ms / 1e3) / 1e9, "steps": n,
+                                "launches_per_step": 2}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    N = 96
+    pk = karma.karma_params(N=N, Fnoise=0.01)
+    o = pyoracle.KarmaOracle(N, N, N, pk.lambda_, pk.eps4, pk.dx, pk.dt, pk.Fnoise, pk.k)
+    o.set(*karma.seed_state(pk))
+    o.step(1)
+    t0, n = time.perf_counter(), 0
+    while n < 3 or time.perf_counter() - t0 < 3.0:
+        o.step(1)
+        n += 1
+    dt = time.perf_counter() - t0
+    out["cpu_baseline"] = {"value": N ** 3 * n / dt / 1e9, "unit": UNIT, "cores": pyoracle.num_threads(),
+                           "kind": "port", "sample": f"{N}^3, {n} steps (C restatement of karma3d.f90, OpenMP)"}
+    return out
+
+
 def bench_serve(args, serve):
     """Bounded sample of the serving configuration (5): the first requests of
     the seeded Poisson stream, every step count scaled by step_scale."""
@@ -255,6 +293,7 @@ def main():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-karma", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--serve-step-scale", type=float, default=0.05)
     args = ap.parse_args()
@@ -383,6 +422,8 @@ def main():
             extra["batched"] = bench_batch(args, pf3d, serve_mod, init)
         if not args.no_serve:
             extra["serving"] = bench_serve(args, serve_mod)
+        if not args.no_karma:
+            extra["karma"] = bench_karma(args, torch, stream)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
