@@ -15,13 +15,15 @@
 //   pass B (karma3d.f90:212-287): U_new from phi, U and dphi (anti-trapping
 //           current through the 6 faces) and phi_new = clamp(phi + dt dphi).
 // Each CTA owns a 32 x TY column tile and marches a z-chunk with rolling
-// shared-memory windows of 3 planes (tile + 1-cell ring).  Every operation
+// shared-memory windows of 4 planes (tile + 1-cell ring): 3 in use while the
+// next is copied in with cp.async.  Every operation
 // is the reference's, in its order, with IEEE division and square root and
 // no contraction: the FP64 result is the reference's arithmetic bit for bit
 // (checked against the C oracle).
 #pragma once
 #include <cstdint>
 #include "pf3d_launch.h"
+#include "pf3d_cpasync.cuh"
 
 namespace pf3d {
 
@@ -77,12 +79,13 @@ __device__ __forceinline__ double k_ruido(int i, int j, int k, int it)
 template <typename T, int TY>
 struct KarmaSmem {
     static constexpr int W = 34, H = TY + 2;
-    T a[3][H][W];
+    T a[4][H][W];
 };
 
 __device__ __forceinline__ int kclamp(int v, int n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); }
 
-// loads plane z (clamped) of f with the 1-cell ring (clamped) into dst
+// issues the asynchronous copy of plane z (clamped) of f with the 1-cell
+// ring (clamped) into dst; the caller commits and waits
 template <typename T, int TY>
 __device__ __forceinline__ void k_load_plane(const KarmaDesc& d, const T* __restrict__ f, int z, int x0, int y0,
                                              T (*dst)[34])
@@ -92,8 +95,8 @@ __device__ __forceinline__ void k_load_plane(const KarmaDesc& d, const T* __rest
     const int tx = threadIdx.x, ty = threadIdx.y;
     for (int ly = ty; ly < TY + 2; ly += TY) {
         const T* row = src + (long long)kclamp(y0 - 1 + ly, d.ny) * d.px;
-        dst[ly][tx] = row[kclamp(x0 - 1 + tx, d.nx)];
-        if (tx < 2) dst[ly][32 + tx] = row[kclamp(x0 + 31 + tx, d.nx)];
+        cp_async_elem(&dst[ly][tx], row + kclamp(x0 - 1 + tx, d.nx), (int)sizeof(T));
+        if (tx < 2) cp_async_elem(&dst[ly][32 + tx], row + kclamp(x0 + 31 + tx, d.nx), (int)sizeof(T));
     }
 }
 
@@ -110,12 +113,20 @@ __global__ void __launch_bounds__(32 * TY) k_karma_phase(KarmaDesc d, const Karm
     const bool own = x < d.nx && y < d.ny;
     const int fx = tx + 1, fy = ty + 1;
     const long long col = (long long)x + (long long)y * d.px;
-    int sm1 = 0, s0 = 1, sp1 = 2;
+    int sm1 = 0, s0 = 1, sp1 = 2, sfree = 3;
     k_load_plane<T, TY>(d, phi, zb - 1, x0, y0, sm.a[sm1]);
     k_load_plane<T, TY>(d, phi, zb, x0, y0, sm.a[s0]);
     k_load_plane<T, TY>(d, phi, zb + 1, x0, y0, sm.a[sp1]);
+    cp_async_commit();
+    T u_next = (own && zb < ze) ? U[col + (long long)zb * d.plane] : (T)0;
+    cp_async_wait_all();
     __syncthreads();
     for (int z = zb; z < ze; ++z) {
+        // plane z+2 lands in the free slot while plane z is computed
+        if (z + 1 < ze) k_load_plane<T, TY>(d, phi, z + 2, x0, y0, sm.a[sfree]);
+        cp_async_commit();
+        const T uc = u_next;
+        if (own && z + 1 < ze) u_next = U[col + (long long)(z + 1) * d.plane];
         if (own) {
             const T(*B)[34] = sm.a[sm1];
             const T(*P)[34] = sm.a[s0];
@@ -157,16 +168,16 @@ __global__ void __launch_bounds__(32 * TY) k_karma_phase(KarmaDesc d, const Karm
             const long long id = col + (long long)z * d.plane;
             const T om = (T)1 - pp * pp;
             const T r = (T)k_ruido(x + 1, y + 1, z + 1, d.it);
-            dphi[id] = (divJ + pp - (pp * pp) * pp - c.lambda * (om * om) * U[id]) / as2 +
+            dphi[id] = (divJ + pp - (pp * pp) * pp - c.lambda * (om * om) * uc) / as2 +
                        c.Fnoise * r * ((T)1 - pp * pp) / c.sqdt;
         }
+        cp_async_wait_all();
         __syncthreads();
         const int t = sm1;
         sm1 = s0;
         s0 = sp1;
-        sp1 = t;
-        if (z + 1 < ze) k_load_plane<T, TY>(d, phi, z + 2, x0, y0, sm.a[sp1]);
-        __syncthreads();
+        sp1 = sfree;
+        sfree = t;
     }
 }
 
@@ -186,9 +197,9 @@ __device__ __forceinline__ T k_uflux(T g1, T g2, T g3, T gn, T pp, T nb, T du, T
 
 template <typename T, int TY>
 struct KarmaSmemB {
-    T p[3][TY + 2][34];
-    T u[3][TY + 2][34];
-    T dp[3][TY + 2][34];
+    T p[4][TY + 2][34];
+    T u[4][TY + 2][34];
+    T dp[4][TY + 2][34];
 };
 
 // pass B: U_new and phi_new of karma3d.f90:212-287
@@ -205,15 +216,24 @@ __global__ void __launch_bounds__(32 * TY) k_karma_solute(KarmaDesc d, const Kar
     const bool own = x < d.nx && y < d.ny;
     const int fx = tx + 1, fy = ty + 1;
     const long long col = (long long)x + (long long)y * d.px;
-    int sm1 = 0, s0 = 1, sp1 = 2;
+    int sm1 = 0, s0 = 1, sp1 = 2, sfree = 3;
     for (int k = -1; k <= 1; ++k) {
         const int sl = k + 1;
         k_load_plane<T, TY>(d, phi, zb + k, x0, y0, sm.p[sl]);
         k_load_plane<T, TY>(d, U, zb + k, x0, y0, sm.u[sl]);
         k_load_plane<T, TY>(d, dphi, zb + k, x0, y0, sm.dp[sl]);
     }
+    cp_async_commit();
+    cp_async_wait_all();
     __syncthreads();
     for (int z = zb; z < ze; ++z) {
+        // plane z+2 lands in the free slots while plane z is computed
+        if (z + 1 < ze) {
+            k_load_plane<T, TY>(d, phi, z + 2, x0, y0, sm.p[sfree]);
+            k_load_plane<T, TY>(d, U, z + 2, x0, y0, sm.u[sfree]);
+            k_load_plane<T, TY>(d, dphi, z + 2, x0, y0, sm.dp[sfree]);
+        }
+        cp_async_commit();
         if (own) {
             const T(*B)[34] = sm.p[sm1];
             const T(*P)[34] = sm.p[s0];
@@ -270,17 +290,13 @@ __global__ void __launch_bounds__(32 * TY) k_karma_solute(KarmaDesc d, const Kar
             const T pn = pp + c.dt * dc;
             phi_out[id] = fmax((T)-1, fmin((T)1, pn));
         }
+        cp_async_wait_all();
         __syncthreads();
         const int t = sm1;
         sm1 = s0;
         s0 = sp1;
-        sp1 = t;
-        if (z + 1 < ze) {
-            k_load_plane<T, TY>(d, phi, z + 2, x0, y0, sm.p[sp1]);
-            k_load_plane<T, TY>(d, U, z + 2, x0, y0, sm.u[sp1]);
-            k_load_plane<T, TY>(d, dphi, z + 2, x0, y0, sm.dp[sp1]);
-        }
-        __syncthreads();
+        sp1 = sfree;
+        sfree = t;
     }
 }
 
