@@ -139,6 +139,9 @@ int pf_set_stream(pf_ctx* ctx, void* stream);
 #define PF_OPT_TILE_Y 2    /* fused tile height: 4, 8 (default) or 16       */
 #define PF_OPT_ZCHUNK 3    /* z planes per fused CTA (0 = whole column)     */
 #define PF_OPT_KTIMING 4   /* 1: time every fused launch with CUDA events   */
+#define PF_OPT_PAIRED 5    /* two cells per thread on 32 x 8 fused tiles
+                              (same results): 1 (default) in FP32, where it
+                              is faster; 2 in both precisions; 0 never      */
 int pf_set_option(pf_ctx* ctx, int opt, int value);
 int pf_get_option(const pf_ctx* ctx, int opt, int* value);
 /* With PF_OPT_KTIMING on: launches and summed device milliseconds of the

@@ -68,7 +68,7 @@ struct pf_ctx {
     std::string ckpt_err;
     cudaStream_t own_stream;
     cudaStream_t stream;
-    int fused, tile_y, zchunk, ktiming;
+    int fused, tile_y, zchunk, ktiming, paired;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_first, ev_last;
     std::string err;
     int device;
@@ -143,6 +143,7 @@ int pf_create(const pf_grid* g, const pf_params* p, int precision, pf_ctx** out)
     ctx->tile_y = 8;
     ctx->zchunk = 64;
     ctx->ktiming = 0;
+    ctx->paired = 1;
     cudaGetDevice(&ctx->device);
     // one allocation: 7 fields + diagnostics partials
     ctx->field_bytes = round_up((size_t)px * g->ny * g->nz * ctx->es + 64, 256);
@@ -246,6 +247,10 @@ int pf_set_option(pf_ctx* ctx, int opt, int value)
         ctx->zchunk = value;
         return PF_OK;
     case PF_OPT_KTIMING: ctx->ktiming = value ? 1 : 0; return PF_OK;
+    case PF_OPT_PAIRED:
+        if (value < 0 || value > 2) return ctx_err(ctx, PF_E_ARG, "paired must be 0, 1 or 2");
+        ctx->paired = value;
+        return PF_OK;
     }
     return ctx_err(ctx, PF_E_ARG, "unknown option");
 }
@@ -258,6 +263,7 @@ int pf_get_option(const pf_ctx* ctx, int opt, int* value)
     case PF_OPT_TILE_Y: *value = ctx->tile_y; return PF_OK;
     case PF_OPT_ZCHUNK: *value = ctx->zchunk; return PF_OK;
     case PF_OPT_KTIMING: *value = ctx->ktiming; return PF_OK;
+    case PF_OPT_PAIRED: *value = ctx->paired; return PF_OK;
     }
     return PF_E_ARG;
 }
@@ -589,12 +595,17 @@ static int one_step(pf_ctx* ctx)
     void* final_phi;
     void* other_phi;
     if (ctx->fused) {
+        // two cells per thread on 32 x 8 tiles; the smooth noise keeps one
+        const bool pair = (ctx->paired == 2 || (ctx->paired == 1 && !is64(ctx))) && ctx->tile_y == 8 &&
+                          p.ruido_tipo != 2 && !ctx->dd.do_heat_lap;
         if (nsw == 1) {
             f.phi_mid = B;
             cudaEvent_t e0 = nullptr, e1 = nullptr;
             if (ctx->ktiming) { e0 = new_event(); e1 = new_event(); cudaEventRecord(e0, ctx->stream); }
-            CK(is64(ctx) ? launch_fused_first<double>(ctx->dd, s, f, true, ctx->tile_y, ctx->zchunk, ctx->stream)
-                         : launch_fused_first<float>(ctx->dd, s, f, true, ctx->tile_y, ctx->zchunk, ctx->stream),
+            CK(pair ? (is64(ctx) ? launch_fused_first_pair<double>(ctx->dd, s, f, true, ctx->zchunk, ctx->stream)
+                                 : launch_fused_first_pair<float>(ctx->dd, s, f, true, ctx->zchunk, ctx->stream))
+                    : (is64(ctx) ? launch_fused_first<double>(ctx->dd, s, f, true, ctx->tile_y, ctx->zchunk, ctx->stream)
+                                 : launch_fused_first<float>(ctx->dd, s, f, true, ctx->tile_y, ctx->zchunk, ctx->stream)),
                "fused step (single sweep)");
             if (ctx->ktiming) { cudaEventRecord(e1, ctx->stream); ctx->ev_first.push_back({e0, e1}); }
             final_phi = B;
@@ -603,8 +614,10 @@ static int one_step(pf_ctx* ctx)
             f.phi_mid = B;
             cudaEvent_t e0 = nullptr, e1 = nullptr;
             if (ctx->ktiming) { e0 = new_event(); e1 = new_event(); cudaEventRecord(e0, ctx->stream); }
-            CK(is64(ctx) ? launch_fused_first<double>(ctx->dd, s, f, false, ctx->tile_y, ctx->zchunk, ctx->stream)
-                         : launch_fused_first<float>(ctx->dd, s, f, false, ctx->tile_y, ctx->zchunk, ctx->stream),
+            CK(pair ? (is64(ctx) ? launch_fused_first_pair<double>(ctx->dd, s, f, false, ctx->zchunk, ctx->stream)
+                                 : launch_fused_first_pair<float>(ctx->dd, s, f, false, ctx->zchunk, ctx->stream))
+                    : (is64(ctx) ? launch_fused_first<double>(ctx->dd, s, f, false, ctx->tile_y, ctx->zchunk, ctx->stream)
+                                 : launch_fused_first<float>(ctx->dd, s, f, false, ctx->tile_y, ctx->zchunk, ctx->stream)),
                "fused heat + sweep 1");
             if (ctx->ktiming) { cudaEventRecord(e1, ctx->stream); ctx->ev_first.push_back({e0, e1}); }
             void* cur = B;   // phase after the sweeps so far
@@ -620,8 +633,10 @@ static int one_step(pf_ctx* ctx)
             f2.phi_mid = cur;
             f2.phi_new = oth;
             if (ctx->ktiming) { e0 = new_event(); e1 = new_event(); cudaEventRecord(e0, ctx->stream); }
-            CK(is64(ctx) ? launch_fused_last<double>(ctx->dd, s, f2, ctx->tile_y, ctx->zchunk, ctx->stream)
-                         : launch_fused_last<float>(ctx->dd, s, f2, ctx->tile_y, ctx->zchunk, ctx->stream),
+            CK(pair ? (is64(ctx) ? launch_fused_last_pair<double>(ctx->dd, s, f2, ctx->zchunk, ctx->stream)
+                                 : launch_fused_last_pair<float>(ctx->dd, s, f2, ctx->zchunk, ctx->stream))
+                    : (is64(ctx) ? launch_fused_last<double>(ctx->dd, s, f2, ctx->tile_y, ctx->zchunk, ctx->stream)
+                                 : launch_fused_last<float>(ctx->dd, s, f2, ctx->tile_y, ctx->zchunk, ctx->stream)),
                "fused last sweep + solute");
             if (ctx->ktiming) { cudaEventRecord(e1, ctx->stream); ctx->ev_last.push_back({e0, e1}); }
             final_phi = oth;

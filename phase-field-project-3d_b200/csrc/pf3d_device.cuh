@@ -14,6 +14,7 @@
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+#include "pf3d_pair.cuh"
 
 namespace pf3d {
 
@@ -157,6 +158,49 @@ template <> struct Ar<float> {
     static __device__ __forceinline__ float lg(float x) { return __logf(x); }
 };
 
+// ---- lane-generic helpers: scalar float / double, and the lane pairs F2 / D2
+// (two cells per thread, pf3d_pair.cuh) with the same per-lane operations ----
+template <typename T> struct IsF64 { static constexpr bool value = false; };
+template <> struct IsF64<double> { static constexpr bool value = true; };
+template <> struct IsF64<D2> { static constexpr bool value = true; };
+
+__device__ __forceinline__ float vabs(float x) { return fabsf(x); }
+__device__ __forceinline__ double vabs(double x) { return fabs(x); }
+__device__ __forceinline__ F2 vabs(F2 x) { F2 r; r.v = x.v & 0x7fffffff7fffffffull; return r; }
+__device__ __forceinline__ D2 vabs(D2 x) { return D2(fabs(x.a), fabs(x.b)); }
+__device__ __forceinline__ float vmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double vmax(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ F2 vmax(F2 a, F2 b) { return F2(fmaxf(a.x(), b.x()), fmaxf(a.y(), b.y())); }
+__device__ __forceinline__ D2 vmax(D2 a, D2 b) { return D2(fmax(a.a, b.a), fmax(a.b, b.b)); }
+// (a < b) ? x : y, (a > b) ? x : y and (a <= b) ? x : y, lane by lane
+template <typename T> __device__ __forceinline__ T sel_lt(T a, T b, T x, T y) { return (a < b) ? x : y; }
+template <typename T> __device__ __forceinline__ T sel_gt(T a, T b, T x, T y) { return (a > b) ? x : y; }
+template <typename T> __device__ __forceinline__ T sel_le(T a, T b, T x, T y) { return (a <= b) ? x : y; }
+#define PF3D_PAIR_SEL(NAME, OP)                                                                          \
+    template <> __device__ __forceinline__ F2 NAME<F2>(F2 a, F2 b, F2 x, F2 y)                          \
+    {                                                                                                    \
+        return F2((a.x() OP b.x()) ? x.x() : y.x(), (a.y() OP b.y()) ? x.y() : y.y());                  \
+    }                                                                                                    \
+    template <> __device__ __forceinline__ D2 NAME<D2>(D2 a, D2 b, D2 x, D2 y)                          \
+    {                                                                                                    \
+        return D2((a.a OP b.a) ? x.a : y.a, (a.b OP b.b) ? x.b : y.b);                                  \
+    }
+PF3D_PAIR_SEL(sel_lt, <)
+PF3D_PAIR_SEL(sel_gt, >)
+PF3D_PAIR_SEL(sel_le, <=)
+#undef PF3D_PAIR_SEL
+
+template <> struct Ar<F2> {
+    static __device__ __forceinline__ F2 rcp(F2 x) { return F2(__fdividef(1.0f, x.x()), __fdividef(1.0f, x.y())); }
+    static __device__ __forceinline__ F2 div(F2 a, F2 b) { return F2(__fdividef(a.x(), b.x()), __fdividef(a.y(), b.y())); }
+    static __device__ __forceinline__ F2 lg(F2 x) { return F2(__logf(x.x()), __logf(x.y())); }
+};
+template <> struct Ar<D2> {
+    static __device__ __forceinline__ D2 rcp(D2 x) { return D2(rcp_nr(x.a), rcp_nr(x.b)); }
+    static __device__ __forceinline__ D2 div(D2 a, D2 b) { return D2(a.a * rcp_nr(b.a), a.b * rcp_nr(b.b)); }
+    static __device__ __forceinline__ D2 lg(D2 x) { return D2(log(x.a), log(x.b)); }
+};
+
 // Explicit multiply-add.  Every translation unit is built without automatic
 // contraction, so the same source gives the same bits in every kernel that
 // inlines it (single domain, batch, any tile shape); the fast form asks for
@@ -231,7 +275,7 @@ __device__ __forceinline__ Node<T> aniso_node(T gx, T gy, T gz, const KC<T>& c)
         n.exy = Ke_ * gx * gy * (gx2 - gy2) / Q2;
         n.eyz = Ke_ * gy * gz * (gy2 - gz2) / Q2;
         n.ezx = Ke_ * gz * gx * (gz2 - gx2) / Q2;
-    } else if constexpr (sizeof(T) == 8) {
+    } else if constexpr (IsF64<T>::value) {
         T Q = fmadd(gx, gx, fmadd(gy, gy, fmadd(gz, gz, (T)1e-23)));
         T S4 = fmadd(gx2, gx2, fmadd(gy2, gy2, gz2 * gz2));
         T rq = Ar<T>::rcp(Q * Q);
@@ -247,7 +291,7 @@ __device__ __forceinline__ Node<T> aniso_node(T gx, T gy, T gz, const KC<T>& c)
         // Clamping m at 1e-15 keeps it branch-free: for smaller gradients the
         // normalised components stay <= 1e-0 and small/m^2 >= 1e7, so the
         // ratio and the cross terms vanish as in the reference.
-        const T m = fmaxf(fmaxf(fabsf(gx), fabsf(gy)), fmaxf(fabsf(gz), (T)1e-15));
+        const T m = vmax(vmax(vabs(gx), vabs(gy)), vmax(vabs(gz), (T)1e-15));
         const T im = Ar<T>::rcp(m);
         const T ux = gx * im, uy = gy * im, uz = gz * im;
         const T ux2 = ux * ux, uy2 = uy * uy, uz2 = uz * uz;
@@ -276,7 +320,7 @@ struct Nbr {
 template <typename T, bool FAST>
 __device__ __forceinline__ T phase_ppnew(const Nbr<T>& p, const Node<T>& E, const Node<T>& W, const Node<T>& N,
                                           const Node<T>& S, const Node<T>& Tt, const Node<T>& B, T CPP,
-                                          float ran, const KC<T>& c)
+                                          T ran, const KC<T>& c)
 {
     const T PP = p.PP;
     const T one = (T)1, two = (T)2;
@@ -345,7 +389,7 @@ __device__ __forceinline__ T phase_ppnew(const Nbr<T>& p, const Node<T>& E, cons
         }
         T den = fmadd(-c.omKe, h, one);
         // (1-CLP)/(1-CSP) = (den - c)/(den - Ke c); the constant factor is in Lc
-        T lg = Ar<T>::lg(fabs(Ar<T>::div(den - CPP, fmadd(-c.Ke, CPP, den)))) + c.Lc;
+        T lg = Ar<T>::lg(vabs(Ar<T>::div(den - CPP, fmadd(-c.Ke, CPP, den)))) + c.Lc;
         T GG = fmadd(c.RTV * h_linha, lg, -(c.W0 * g_linha));
         T pp2q2 = PP * PP * q * q * c.AAA16;
         T ruidos = (c.rt == 0) ? (T)ran * pp2q2 : fmadd(two, (T)ran, -one) * pp2q2;
@@ -357,8 +401,9 @@ __device__ __forceinline__ T phase_ppnew(const Nbr<T>& p, const Node<T>& E, cons
 template <typename T>
 __device__ __forceinline__ T clamp01(T x)
 {
-    T t = (x < (T)1) ? x : (T)1;
-    return (t > (T)0) ? t : (T)0;
+    const T one = (T)1, zero = (T)0;
+    T t = sel_lt(x, one, x, one);
+    return sel_gt(t, zero, t, zero);
 }
 
 // h(phi) as written in conc_body.inc:42-58 (note the quintic form differs
@@ -403,7 +448,7 @@ __device__ __forceinline__ T conc_new(T PP, T CPP, const SolNode<T>& P, const So
                                       const SolNode<T>& N, const SolNode<T>& S, const SolNode<T>& Tt,
                                       const SolNode<T>& B, const KC<T>& c)
 {
-    const T Dc = (PP <= (T)0.95) ? c.D_liq : c.D_sol;
+    const T Dc = sel_le(PP, (T)0.95, c.D_liq, c.D_sol);
     const T two = (T)2;
     if constexpr (!FAST) {
         T GP = Dc * P.br, GS = Dc * S.br, GN = Dc * N.br, GW = Dc * W.br, GE = Dc * E.br, GT = Dc * Tt.br,
@@ -421,10 +466,10 @@ __device__ __forceinline__ T conc_new(T PP, T CPP, const SolNode<T>& P, const So
                CPP;
     } else {
         // 2/(1/(Dc a) + 1/(Dc b)) = 2 Dc a b / (a + b)
-        const T D2 = two * Dc * P.br;
+        const T Dab = two * Dc * P.br;
         auto hm = [&](T b) -> T {
             T sum = P.br + b;
-            return (sum > (T)0) ? D2 * b * Ar<T>::rcp(sum) : (T)0;
+            return sel_gt(sum, (T)0, Dab * b * Ar<T>::rcp(sum), (T)0);
         };
         T fx = fmadd(hm(E.br), E.mu - P.mu, -(hm(W.br) * (P.mu - W.mu)));
         T fy = fmadd(hm(N.br), N.mu - P.mu, -(hm(S.br) * (P.mu - S.mu)));
@@ -433,8 +478,9 @@ __device__ __forceinline__ T conc_new(T PP, T CPP, const SolNode<T>& P, const So
     }
 }
 
-// temp_body.inc:31-41 at an interior cell.
-template <typename T>
+// temp_body.inc:31-41 at an interior cell.  LAP = false compiles only the
+// D = 0 form (for kernels that run on decks without heat diffusion).
+template <typename T, bool LAP = true>
 __device__ __forceinline__ T heat_new(T PP, T dpp, T TE, T TW, T TN, T TS, T TT, T TB, const KC<T>& c)
 {
     T h_linha;
@@ -443,7 +489,7 @@ __device__ __forceinline__ T heat_new(T PP, T dpp, T TE, T TW, T TN, T TS, T TT,
     else
         h_linha = (T)2 * PP * ((T)3 - (T)2 * PP) - (T)2 * PP * PP;
     T FONTE = c.dH_cp * h_linha * dpp;
-    if (c.lap) {
+    if (LAP && c.lap) {
         T TP = c.TP_heat;
         T lap = ((TE - (T)2 * TP + TW) / c.dx2) + ((TN - (T)2 * TP + TS) / c.dy2) + ((TT - (T)2 * TP + TB) / c.dz2);
         return c.Ddt * lap + FONTE + TP;

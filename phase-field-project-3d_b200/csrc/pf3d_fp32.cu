@@ -5,6 +5,7 @@
 #include "pf3d_track.cuh"
 #include "pf3d_frame.cuh"
 #include "pf3d_fused.cuh"
+#include "pf3d_fused_pair.cuh"
 
 namespace pf3d {
 template cudaError_t launch_heat<float>(const DomainDesc&, const StepArgs&, const Fields&, cudaStream_t);
@@ -40,4 +41,6 @@ cudaError_t launch_fill<float>(void* a, long long n, double v, cudaStream_t st)
 {
     return launch_fill_impl<float>(a, n, v, st);
 }
+template cudaError_t launch_fused_first_pair<float>(const DomainDesc&, const StepArgs&, const Fields&, bool, int, cudaStream_t);
+template cudaError_t launch_fused_last_pair<float>(const DomainDesc&, const StepArgs&, const Fields&, int, cudaStream_t);
 }  // namespace pf3d

@@ -35,6 +35,11 @@ template <typename T> cudaError_t launch_copy_inner(const DomainDesc& d, const v
 //   buffer for the last pass; sweeps in between must not write DPP.
 template <typename T> cudaError_t launch_fused_first(const DomainDesc& d, const StepArgs& s, const Fields& f,
                                                      bool with_solute, int tile_y, int zchunk, cudaStream_t st);
+// the same passes with two cells per thread (32 x 8 tiles, no smooth noise)
+template <typename T> cudaError_t launch_fused_first_pair(const DomainDesc& d, const StepArgs& s, const Fields& f,
+                                                          bool with_solute, int zchunk, cudaStream_t st);
+template <typename T> cudaError_t launch_fused_last_pair(const DomainDesc& d, const StepArgs& s, const Fields& f,
+                                                         int zchunk, cudaStream_t st);
 template <typename T> cudaError_t launch_fused_last(const DomainDesc& d, const StepArgs& s, const Fields& f,
                                                     int tile_y, int zchunk, cudaStream_t st);
 

@@ -1,0 +1,88 @@
+// pf3d_pair.cuh -- lane-pair arithmetic: two cells per thread.
+//
+// F2 holds two floats in one 64-bit register pair.  Its explicit multiply-add
+// is Blackwell's packed fma.rn.f32x2 (sm_100a): one instruction, the same
+// IEEE fused operation on both cells.  Products, sums and differences stay
+// one scalar instruction per lane: ptxas contracts a packed mul.rn.f32x2 that
+// feeds a packed add.rn.f32x2 into a packed fma even under --fmad=false
+// (measured on B200: 15 % of random operands round differently), which would
+// break the rule that nothing is contracted unless asked for.  D2 holds two
+// doubles and does each operation once per lane.  Every operation is the
+// scalar one per lane, so a cell computed in a pair has the bits it has when
+// computed alone.
+#pragma once
+#include <cstdint>
+#include <cstring>
+
+namespace pf3d {
+
+struct F2 {
+    unsigned long long v;
+    __host__ __device__ __forceinline__ F2() {}
+    // both lanes = a (host or device)
+    static __host__ __device__ __forceinline__ F2 splat(float a)
+    {
+        unsigned u;
+        memcpy(&u, &a, 4);
+        F2 r;
+        r.v = ((unsigned long long)u << 32) | u;
+        return r;
+    }
+    __device__ __forceinline__ explicit F2(float a) { asm("mov.b64 %0, {%1, %1};" : "=l"(v) : "f"(a)); }
+    __device__ __forceinline__ F2(float a, float b) { asm("mov.b64 %0, {%1, %2};" : "=l"(v) : "f"(a), "f"(b)); }
+    __device__ __forceinline__ float x() const { float a, b; asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); (void)b; return a; }
+    __device__ __forceinline__ float y() const { float a, b; asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); (void)a; return b; }
+    __device__ __forceinline__ float lane(int i) const { return i ? y() : x(); }
+};
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return F2(__fadd_rn(a.x(), b.x()), __fadd_rn(a.y(), b.y())); }
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return F2(__fsub_rn(a.x(), b.x()), __fsub_rn(a.y(), b.y())); }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return F2(__fmul_rn(a.x(), b.x()), __fmul_rn(a.y(), b.y())); }
+// exact negation: flip both sign bits
+__device__ __forceinline__ F2 operator-(F2 a) { F2 r; r.v = a.v ^ 0x8000000080000000ull; return r; }
+__device__ __forceinline__ F2 fmadd(F2 a, F2 b, F2 c) { F2 r; asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v)); return r; }
+__device__ __forceinline__ F2 operator/(F2 a, F2 b) { return F2(a.x() / b.x(), a.y() / b.y()); }
+
+struct D2 {
+    double a, b;
+    __host__ __device__ __forceinline__ D2() {}
+    static __host__ __device__ __forceinline__ D2 splat(double s)
+    {
+        D2 r;
+        r.a = s;
+        r.b = s;
+        return r;
+    }
+    __device__ __forceinline__ explicit D2(double s) : a(s), b(s) {}
+    __device__ __forceinline__ D2(double p, double q) : a(p), b(q) {}
+    __device__ __forceinline__ double x() const { return a; }
+    __device__ __forceinline__ double y() const { return b; }
+    __device__ __forceinline__ double lane(int i) const { return i ? b : a; }
+};
+__device__ __forceinline__ D2 operator+(D2 p, D2 q) { return D2(__dadd_rn(p.a, q.a), __dadd_rn(p.b, q.b)); }
+__device__ __forceinline__ D2 operator-(D2 p, D2 q) { return D2(__dsub_rn(p.a, q.a), __dsub_rn(p.b, q.b)); }
+__device__ __forceinline__ D2 operator*(D2 p, D2 q) { return D2(__dmul_rn(p.a, q.a), __dmul_rn(p.b, q.b)); }
+__device__ __forceinline__ D2 operator-(D2 p) { return D2(-p.a, -p.b); }
+__device__ __forceinline__ D2 fmadd(D2 p, D2 q, D2 r) { return D2(__fma_rn(p.a, q.a, r.a), __fma_rn(p.b, q.b, r.b)); }
+__device__ __forceinline__ D2 operator/(D2 p, D2 q) { return D2(__ddiv_rn(p.a, q.a), __ddiv_rn(p.b, q.b)); }
+
+// scalar type of a lane pair
+template <typename V> struct LaneOf;
+template <> struct LaneOf<F2> { using type = float; };
+template <> struct LaneOf<D2> { using type = double; };
+// lane-pair type of a scalar
+template <typename S> struct PairOf;
+template <> struct PairOf<float> { using type = F2; };
+template <> struct PairOf<double> { using type = D2; };
+
+template <typename V, typename F>
+__device__ __forceinline__ V lanewise(V a, F f)
+{
+    return V(f(a.x()), f(a.y()));
+}
+template <typename V, typename F>
+__device__ __forceinline__ V lanewise2(V a, V b, F f)
+{
+    return V(f(a.x(), b.x()), f(a.y(), b.y()));
+}
+
+}  // namespace pf3d

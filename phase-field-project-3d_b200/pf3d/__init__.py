@@ -19,7 +19,7 @@ from . import _abi
 from ._abi import (LIB, check, pf_grid, pf_params, pf_derived, pf_state, PFError,
                    PF_FP64, PF_FP32, PF_PHASE_OLD, PF_PHASE_NEW, PF_CONC_OLD, PF_CONC_NEW,
                    PF_TOLD, PF_TNEW, PF_DPP, PF_OPT_FUSED, PF_OPT_TILE_Y, PF_OPT_ZCHUNK,
-                   PF_OPT_KTIMING, FIELD_NAMES)
+                   PF_OPT_KTIMING, PF_OPT_PAIRED, FIELD_NAMES)
 from .deck import run6_params, params_copy, grid, read_entrada, WORKLOADS, Workload
 
 __all__ = ["Domain", "PFError", "run6_params", "params_copy", "grid", "read_entrada", "WORKLOADS", "Workload",

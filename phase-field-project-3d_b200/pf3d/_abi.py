@@ -16,7 +16,7 @@ PF_PHASE_OLD, PF_PHASE_NEW, PF_CONC_OLD, PF_CONC_NEW, PF_TOLD, PF_TNEW, PF_DPP =
 FIELD_NAMES = ("phase_field_old", "phase_field_new", "conc_soluto_old", "conc_soluto_new", "TOLD", "TNEW", "DPP")
 PF_FP64, PF_FP32 = 64, 32
 PF_BC_REFERENCE = 0
-PF_OPT_FUSED, PF_OPT_TILE_Y, PF_OPT_ZCHUNK, PF_OPT_KTIMING = 1, 2, 3, 4
+PF_OPT_FUSED, PF_OPT_TILE_Y, PF_OPT_ZCHUNK, PF_OPT_KTIMING, PF_OPT_PAIRED = 1, 2, 3, 4, 5
 PF_NOALLOC_MAX_PLANES = 4096
 
 
