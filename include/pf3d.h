@@ -289,8 +289,12 @@ int pf_batch_step(pf_batch* b, int n_steps);
 /* device milliseconds of the last pf_batch_step call (all its graphs)      */
 double pf_batch_last_ms(const pf_batch* b);
 int pf_batch_set_tile(pf_batch* b, int tile_y, int zchunk);
+/* FP32 batches on 32 x 8 tiles: 1 runs two cells per thread (same results),
+   0 one; batches with the smooth noise or heat diffusion always run one    */
+int pf_batch_set_paired(pf_batch* b, int paired);
 /* Autotuner: times every tile height (4, 8, 16) x z-chunk (16, 32, 64, 128)
-   on real steps (the results do not depend on the tile shape; each candidate
+   -- and in FP32, for 32 x 8 tiles, one or two cells per thread -- on real
+   steps (the results do not depend on these choices; each candidate
    advances the batch by 1 + steps_per_candidate steps), keeps the fastest
    and caches it per shape class (precision, median column size and depth) */
 int pf_batch_autotune(pf_batch* b, int steps_per_candidate, int* tile_y, int* zchunk, double* ms_per_step);

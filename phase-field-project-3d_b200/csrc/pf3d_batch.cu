@@ -54,7 +54,7 @@ struct Slot {
 
 // autotuner cache: shape class -> (tile_y, zchunk)
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int>, std::pair<int, int>> g_tune_cache;
+std::map<std::tuple<int, int, int>, std::tuple<int, int, int>> g_tune_cache;   // -> tile_y, zchunk, pair
 
 }  // namespace
 
@@ -80,10 +80,11 @@ struct pf_batch {
     double* h_out = nullptr;
     double* d_sites = nullptr;         // bump sites for device initialisation
     int tile_y = 8, zchunk = 64, n_sm = 0;   // persistent grids: n_sm x resident CTAs
+    int pair = 0;                      // FP32 32 x 8 tiles with two cells per thread (set by the autotuner)
     cudaStream_t own_stream = nullptr, stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graph_ty = 0, graph_zc = 0, graph_nsm = 0, graph_nsw = 0;
-    bool graph_smooth = false;
+    bool graph_smooth = false, graph_pair = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
     long long last_steps = 0;
@@ -152,11 +153,23 @@ static bool any_smooth(const pf_batch* b)
     return false;
 }
 
+// whether any domain of the batch diffuses heat (D > 0)
+static bool any_lap(const pf_batch* b)
+{
+    for (const Slot& sl : b->slots)
+        if (sl.used && sl.p.D != 0.0) return true;
+    return false;
+}
+
 static int capture_graph(pf_batch* b)
 {
     const bool smooth = any_smooth(b);
+    // two cells per thread: FP32 batches on 32 x 8 tiles whose decks allow it,
+    // when the autotuner measured it faster (boundary tiles, frequent in
+    // small domains, run the one-cell code twice per thread)
+    const bool pair = b->pair && !b64(b) && b->tile_y == 8 && !smooth && !any_lap(b);
     if (b->graph && b->graph_ty == b->tile_y && b->graph_zc == b->zchunk && b->graph_nsm == b->n_sm &&
-        b->graph_nsw == b->nsw && b->graph_smooth == smooth)
+        b->graph_nsw == b->nsw && b->graph_smooth == smooth && b->graph_pair == pair)
         return PF_OK;
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
@@ -170,6 +183,14 @@ static int capture_graph(pf_batch* b)
         for (int k = 0; k < kGraphSteps && e == cudaSuccess; ++k) {
             const BatchStep* st = b->d_steps + (size_t)k * b->max_domains;
             const bool one = b->nsw == 1;
+            if (pair) {
+                e = launch_fused_batch_pair<float>(b->d_doms, st, b->d_items, b->d_nitems, 0, one, b->zchunk, b->n_sm,
+                                                   cs);
+                if (e == cudaSuccess && !one)
+                    e = launch_fused_batch_pair<float>(b->d_doms, st, b->d_items, b->d_nitems, 1, false, b->zchunk,
+                                                       b->n_sm, cs);
+                continue;
+            }
             e = b64(b) ? launch_fused_batch<double>(b->d_doms, st, b->d_items, b->d_nitems, 0, one, smooth, b->tile_y,
                                                     b->zchunk, b->n_sm, cs)
                        : launch_fused_batch<float>(b->d_doms, st, b->d_items, b->d_nitems, 0, one, smooth, b->tile_y,
@@ -192,6 +213,7 @@ static int capture_graph(pf_batch* b)
     b->graph_nsm = b->n_sm;
     b->graph_nsw = b->nsw;
     b->graph_smooth = smooth;
+    b->graph_pair = pair;
     return PF_OK;
 }
 
@@ -521,6 +543,13 @@ int pf_batch_get_state(const pf_batch* b, int slot, pf_state* out)
     return PF_OK;
 }
 
+int pf_batch_set_paired(pf_batch* b, int paired)
+{
+    if (!b || paired < 0 || paired > 1) return berr(b, PF_E_ARG, "pf_batch_set_paired: 0 or 1");
+    b->pair = paired;
+    return PF_OK;
+}
+
 int pf_batch_set_tile(pf_batch* b, int tile_y, int zchunk)
 {
     if (!b || (tile_y != 4 && tile_y != 8 && tile_y != 16) || zchunk < 1)
@@ -593,9 +622,10 @@ int pf_batch_autotune(pf_batch* b, int steps_per_candidate, int* tile_y, int* zc
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) {
-            int rc = pf_batch_set_tile(b, it->second.first, it->second.second);
-            if (tile_y) *tile_y = it->second.first;
-            if (zchunk) *zchunk = it->second.second;
+            int rc = pf_batch_set_tile(b, std::get<0>(it->second), std::get<1>(it->second));
+            b->pair = std::get<2>(it->second);
+            if (tile_y) *tile_y = std::get<0>(it->second);
+            if (zchunk) *zchunk = std::get<1>(it->second);
             if (ms_per_step) *ms_per_step = -1.0;
             return rc;
         }
@@ -603,25 +633,29 @@ int pf_batch_autotune(pf_batch* b, int steps_per_candidate, int* tile_y, int* zc
     // every candidate runs real steps (results do not depend on the tile
     // shape), one untimed step first
     double best = 1e300;
-    int bty = b->tile_y, bzc = b->zchunk;
+    int bty = b->tile_y, bzc = b->zchunk, bpair = 0;
     for (int ty : {4, 8, 16})
-        for (int zc : {16, 32, 64, 128}) {
-            int rc = pf_batch_set_tile(b, ty, zc);
-            if (!rc) rc = pf_batch_step(b, 1);
-            if (!rc) rc = pf_batch_step(b, steps_per_candidate);
-            if (rc) return rc;
-            if (b->last_steps == 0) break;
-            const double ms = b->last_ms / (double)b->last_steps;
-            if (ms < best) {
-                best = ms;
-                bty = ty;
-                bzc = zc;
+        for (int zc : {16, 32, 64, 128})
+            for (int pr = 0; pr <= ((ty == 8 && !b64(b)) ? 1 : 0); ++pr) {
+                int rc = pf_batch_set_tile(b, ty, zc);
+                b->pair = pr;
+                if (!rc) rc = pf_batch_step(b, 1);
+                if (!rc) rc = pf_batch_step(b, steps_per_candidate);
+                if (rc) return rc;
+                if (b->last_steps == 0) break;
+                const double ms = b->last_ms / (double)b->last_steps;
+                if (ms < best) {
+                    best = ms;
+                    bty = ty;
+                    bzc = zc;
+                    bpair = pr;
+                }
             }
-        }
     int rc = pf_batch_set_tile(b, bty, bzc);
+    b->pair = bpair;
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
-        g_tune_cache[key] = {bty, bzc};
+        g_tune_cache[key] = std::make_tuple(bty, bzc, bpair);
     }
     if (tile_y) *tile_y = bty;
     if (zchunk) *zchunk = bzc;

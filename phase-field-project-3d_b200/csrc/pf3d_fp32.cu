@@ -43,4 +43,5 @@ cudaError_t launch_fill<float>(void* a, long long n, double v, cudaStream_t st)
 }
 template cudaError_t launch_fused_first_pair<float>(const DomainDesc&, const StepArgs&, const Fields&, bool, int, cudaStream_t);
 template cudaError_t launch_fused_last_pair<float>(const DomainDesc&, const StepArgs&, const Fields&, int, cudaStream_t);
+template cudaError_t launch_fused_batch_pair<float>(const BatchDomain*, const BatchStep*, const BatchItem*, const int*, int, bool, int, int, cudaStream_t);
 }  // namespace pf3d

@@ -10,4 +10,5 @@ template cudaError_t launch_fused_last<double>(const DomainDesc&, const StepArgs
 template cudaError_t launch_fused_batch<double>(const BatchDomain*, const BatchStep*, const BatchItem*, const int*, int, bool, bool, int, int, int, cudaStream_t);
 template cudaError_t launch_fused_first_pair<double>(const DomainDesc&, const StepArgs&, const Fields&, bool, int, cudaStream_t);
 template cudaError_t launch_fused_last_pair<double>(const DomainDesc&, const StepArgs&, const Fields&, int, cudaStream_t);
+template cudaError_t launch_fused_batch_pair<double>(const BatchDomain*, const BatchStep*, const BatchItem*, const int*, int, bool, int, int, cudaStream_t);
 }  // namespace pf3d

@@ -500,3 +500,89 @@ cudaError_t launch_fused_last_pair(const DomainDesc& d, const StepArgs& s, const
 }
 
 }  // namespace pf3d
+
+namespace pf3d {
+
+// many domains, two cells per thread: the persistent work-list kernel of
+// k_fused_batch with fused_tile_pair (PASS 0 first pass, 1 last pass)
+template <typename S, int TY, int PASS, bool ONE_SWEEP>
+__global__ void __launch_bounds__(16 * TY, (PairOcc<S, PASS == 0>::v))
+    k_fused_batch_pair(const BatchDomain* __restrict__ doms, const BatchStep* __restrict__ steps,
+                       const BatchItem* __restrict__ items, const int* __restrict__ n_items, int zchunk)
+{
+    using V = typename PairOf<S>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(16) KC<S> skc;   // the loop constants of the current item
+    __shared__ __align__(16) KC<V> skv;   // the same, broadcast to both lanes
+    constexpr int nf = (int)(offsetof(KC<S>, hq) / sizeof(S));
+    const int n = *n_items;
+    const int tid = threadIdx.x + 32 * threadIdx.y;
+    for (int w = blockIdx.x; w < n; w += gridDim.x) {
+        const BatchItem it = items[w];
+        const BatchStep& st = steps[it.dom];
+        if (!st.active) continue;   // uniform across the CTA
+        const BatchDomain& D = doms[it.dom];
+        const int q = st.q_phi, qc = st.q_c, qt = st.q_T;
+        static_assert(sizeof(KC<S>) % 4 == 0, "KC is copied as words");
+        for (int i = tid; i < (int)(sizeof(KC<S>) / 4); i += 16 * TY)
+            reinterpret_cast<int*>(&skc)[i] = reinterpret_cast<const int*>(st.kc)[i];
+        __syncthreads();
+        for (int i = tid; i < nf; i += 16 * TY) reinterpret_cast<V*>(&skv)[i] = V::splat(reinterpret_cast<const S*>(&skc)[i]);
+        if (tid == 0) {
+            skv.hq = skc.hq;
+            skv.rt = skc.rt;
+            skv.it = skc.it;
+            skv.lap = skc.lap;
+        }
+        __syncthreads();
+        if (PASS == 0) {
+            if (ONE_SWEEP)
+                fused_tile_pair<S, TY, true, true, true>(D.d, skc, skv, (const S*)D.phi[q], (const S*)D.c[qc],
+                                                         (S*)D.phi[1 - q], (S*)D.dpp, (S*)D.c[1 - qc],
+                                                         (const S*)D.T[qt], (S*)D.T[1 - qt], zchunk, it.bx, it.by,
+                                                         it.bz, smem_raw);
+            else
+                fused_tile_pair<S, TY, true, false, false>(D.d, skc, skv, (const S*)D.phi[q], (const S*)D.c[qc],
+                                                           (S*)D.phi[1 - q], (S*)D.dpp, nullptr, (const S*)D.T[qt],
+                                                           (S*)D.T[1 - qt], zchunk, it.bx, it.by, it.bz, smem_raw);
+        } else {
+            fused_tile_pair<S, TY, false, true, true>(D.d, skc, skv, (const S*)D.phi[1 - q], (const S*)D.c[qc],
+                                                      (S*)D.phi[q], (S*)D.dpp, (S*)D.c[1 - qc], nullptr, nullptr,
+                                                      zchunk, it.bx, it.by, it.bz, smem_raw);
+        }
+    }
+}
+
+template <typename S, int PASS, bool ONE_SWEEP>
+cudaError_t launch_batch_pair_t(const BatchDomain* doms, const BatchStep* steps, const BatchItem* items,
+                                const int* n_items, int zchunk, int n_sm, cudaStream_t st)
+{
+    auto kern = k_fused_batch_pair<S, 8, PASS, ONE_SWEEP>;
+    const size_t smem = fused_smem_bytes<S, 8>();
+    static int per_sm = 0;   // one attribute and occupancy query per instantiation
+    if (per_sm == 0) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        int nb = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 128, smem);
+        if (e != cudaSuccess) return e;
+        per_sm = nb > 0 ? nb : 1;
+    }
+    kern<<<n_sm * per_sm, dim3(32, 4), smem, st>>>(doms, steps, items, n_items, zchunk);
+    return cudaGetLastError();
+}
+
+// a batch pass with two cells per thread (32 x 8 tiles; batches without the
+// smooth noise and without heat diffusion)
+template <typename S>
+cudaError_t launch_fused_batch_pair(const BatchDomain* doms, const BatchStep* steps, const BatchItem* items,
+                                    const int* n_items, int pass, bool one_sweep, int zchunk, int n_sm,
+                                    cudaStream_t st)
+{
+    if (pass == 0)
+        return one_sweep ? launch_batch_pair_t<S, 0, true>(doms, steps, items, n_items, zchunk, n_sm, st)
+                         : launch_batch_pair_t<S, 0, false>(doms, steps, items, n_items, zchunk, n_sm, st);
+    return launch_batch_pair_t<S, 1, false>(doms, steps, items, n_items, zchunk, n_sm, st);
+}
+
+}  // namespace pf3d

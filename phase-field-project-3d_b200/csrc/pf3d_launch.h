@@ -68,6 +68,11 @@ template <typename T> cudaError_t launch_fused_batch(const BatchDomain* doms, co
                                                      const BatchItem* items, const int* n_items, int pass,
                                                      bool one_sweep, bool smooth, int tile_y, int zchunk,
                                                      int n_sm, cudaStream_t st);
+// the batch passes with two cells per thread (32 x 8 tiles, no smooth noise,
+// no heat diffusion)
+template <typename T> cudaError_t launch_fused_batch_pair(const BatchDomain* doms, const BatchStep* steps,
+                                                          const BatchItem* items, const int* n_items, int pass,
+                                                          bool one_sweep, int zchunk, int n_sm, cudaStream_t st);
 
 // Solidification tracking of phi: out[3] = {solid fraction, tip position
 // (cells, 1-based), solid cells}; scratch holds nz + 1 words.

@@ -331,6 +331,9 @@ class Batch:
     def set_tile(self, tile_y: int, zchunk: int):
         self._chk(LIB.pf_batch_set_tile(self._h, tile_y, zchunk))
 
+    def set_paired(self, paired: int):
+        self._chk(LIB.pf_batch_set_paired(self._h, int(paired)))
+
     def autotune(self, steps_per_candidate: int = 2):
         ty, zc, ms = C.c_int(), C.c_int(), C.c_double()
         self._chk(LIB.pf_batch_autotune(self._h, steps_per_candidate, C.byref(ty), C.byref(zc), C.byref(ms)))

@@ -115,6 +115,7 @@ SIGNATURES = [
     ("pf_batch_step", C.c_int, [_P, C.c_int]),
     ("pf_batch_last_ms", C.c_double, [_P]),
     ("pf_batch_set_tile", C.c_int, [_P, C.c_int, C.c_int]),
+    ("pf_batch_set_paired", C.c_int, [_P, C.c_int]),
     ("pf_batch_autotune", C.c_int, [_P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _D]),
     ("pf_batch_diagnosticos", C.c_int, [_P, C.c_int, _D]),
     ("pf_batch_track", C.c_int, [_P, C.c_int, _D]),

@@ -50,6 +50,25 @@ def test_batch_equals_alone(gpu, prec):
                 assert np.array_equal(got[k], want[k]), (s, k)
 
 
+def test_paired_batch_equals_alone(gpu):
+    """FP32 batch with two cells per thread: every domain keeps its alone bits
+    (domains big enough to have interior tiles, and small ragged ones)."""
+    cases = [case(100, 70, 40), case(40, 33, 50), case(75, 90, 24, h_quintico=1)]
+    with pf3d.Batch(pf3d.PF_FP32) as b:
+        b.set_paired(1)
+        slots = []
+        for g, p, st in cases:
+            s = b.add(g, p)
+            b.load_state(s, st)
+            slots.append(s)
+        b.step(9)
+        for (g, p, st), s in zip(cases, slots):
+            want, _ = alone(g, p, st, pf3d.PF_FP32, 9)
+            got = b.fields(s)
+            for k in want:
+                assert np.array_equal(got[k], want[k]), (s, k)
+
+
 @pytest.mark.parametrize("prec", [pf3d.PF_FP64, pf3d.PF_FP32])
 def test_batch_mixed_noise_kinds(gpu, prec):
     """A batch whose domains draw different noise (the smooth noise selects the
@@ -123,7 +142,9 @@ def test_autotune_keeps_results(gpu):
         ty, zc, ms = b.autotune(1)
         assert ty in (4, 8, 16) and zc in (16, 32, 64, 128)
         n = b.state(slots[0]).it
-        assert n == 24           # 12 candidates x (1 warm-up + 1 timed) real steps
+        # 12 tile shapes + 4 two-cells-per-thread candidates (FP32, 32 x 8)
+        # x (1 warm-up + 1 timed) real steps
+        assert n == 32
         b.step(2)
         for (g, p, st), s in zip(cases, slots):
             want, _ = alone(g, p, st, pf3d.PF_FP32, n + 2)
