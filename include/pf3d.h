@@ -286,6 +286,11 @@ int pf_batch_set_target(pf_batch* b, int slot, long long target_it);
 int pf_batch_get_state(const pf_batch* b, int slot, pf_state* out);
 /* advance every active slot by up to n_steps steps                        */
 int pf_batch_step(pf_batch* b, int n_steps);
+/* the same without waiting: the steps are queued on the batch's stream (the
+   host state of every slot is already advanced); pf_batch_wait waits for
+   them.  Two batches on their own streams so run at the same time.        */
+int pf_batch_step_async(pf_batch* b, int n_steps);
+int pf_batch_wait(pf_batch* b);
 /* device milliseconds of the last pf_batch_step call (all its graphs)      */
 double pf_batch_last_ms(const pf_batch* b);
 int pf_batch_set_tile(pf_batch* b, int tile_y, int zchunk);

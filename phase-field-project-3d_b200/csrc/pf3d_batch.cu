@@ -87,6 +87,7 @@ struct pf_batch {
     bool graph_smooth = false, graph_pair = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
+    bool pending = false;              // steps enqueued by pf_batch_step_async not yet waited for
     long long last_steps = 0;
     std::string err;
 };
@@ -313,6 +314,19 @@ int pf_batch_create(int precision, long long budget_bytes, int max_domains, pf_b
         return set_last_error_global(PF_E_CUDA, std::string("pf_batch_create: ") + cudaGetErrorString(e));
     }
     b->stream = b->own_stream;
+    // slots come from the device's stream-ordered pool (cudaMallocAsync):
+    // adding and removing a domain then neither waits for the GPU nor stops
+    // it; up to 8 GB of freed slot memory stays cached for the next ones
+    {
+        int dev = 0;
+        cudaMemPool_t pool;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t keep = 8ull << 30, cur = 0;
+            if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &cur) == cudaSuccess && cur < keep)
+                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
+    }
     cudaMemset(b->d_steps, 0, step_bytes);
     cudaMemset(b->d_nitems, 0, sizeof(int));
     set_grid(b);
@@ -383,10 +397,10 @@ int pf_batch_add(pf_batch* b, const pf_grid* g, const pf_params* p, int* slot)
     Slot& sl = b->slots[s];
     sl = Slot();
     void* mem = nullptr;
-    cudaError_t e = cudaMalloc(&mem, bytes);
+    cudaError_t e = cudaMallocAsync(&mem, bytes, b->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        return berr(b, PF_E_NOMEM, std::string("pf_batch_add: cudaMalloc: ") + cudaGetErrorString(e));
+        return berr(b, PF_E_NOMEM, std::string("pf_batch_add: cudaMallocAsync: ") + cudaGetErrorString(e));
     }
     cudaMemsetAsync(mem, 0, bytes, b->stream);
     sl.used = true;
@@ -409,8 +423,8 @@ int pf_batch_add(pf_batch* b, const pf_grid* g, const pf_params* p, int* slot)
     sl.bd.T[0] = m + 4 * fb;
     sl.bd.T[1] = m + 5 * fb;
     sl.bd.dpp = m + 6 * fb;
+    // from pageable memory: staged at the call, so no wait is needed
     BCK(cudaMemcpyAsync(b->d_doms + s, &sl.bd, sizeof(BatchDomain), cudaMemcpyHostToDevice, b->stream), "descriptor");
-    BCK(cudaStreamSynchronize(b->stream), "descriptor sync");
     b->used_bytes += (long long)bytes;
     b->nsw = p->n_varreduras;
     b->items_dirty = true;
@@ -422,9 +436,9 @@ int pf_batch_remove(pf_batch* b, int slot)
 {
     if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used)
         return berr(b, PF_E_ARG, "pf_batch_remove: bad slot");
-    BCK(cudaStreamSynchronize(b->stream), "remove sync");
     Slot& sl = b->slots[slot];
-    cudaFree(sl.mem);
+    // stream-ordered: released after the steps already queued that use it
+    BCK(cudaFreeAsync(sl.mem, b->stream), "remove");
     b->used_bytes -= (long long)sl.bytes;
     sl = Slot();
     b->items_dirty = true;
@@ -563,18 +577,21 @@ int pf_batch_set_tile(pf_batch* b, int tile_y, int zchunk)
     return PF_OK;
 }
 
-int pf_batch_step(pf_batch* b, int n_steps)
+// Enqueues up to n_steps steps as graphs of kGraphSteps steps; the host fills
+// the next step table while the GPU runs the current graph (two tables,
+// reused after their upload has completed).  Returns without waiting.
+int pf_batch_step_async(pf_batch* b, int n_steps)
 {
-    if (!b || n_steps < 0) return berr(b, PF_E_ARG, "pf_batch_step: bad argument");
+    if (!b || n_steps < 0) return berr(b, PF_E_ARG, "pf_batch_step_async: bad argument");
     if (b->items_dirty) {
         int rc = rebuild_items(b);
         if (rc) return rc;
     }
     int rc = capture_graph(b);
     if (rc) return rc;
-    double ms_total = 0.0;
     long long steps_done = 0;
     int left = n_steps;
+    bool launched = false;
     while (left > 0) {
         const int chunk = std::min(left, kGraphSteps);
         const int hb = b->h_cur;
@@ -587,18 +604,37 @@ int pf_batch_step(pf_batch* b, int n_steps)
             "step table upload");
         BCK(cudaEventRecord(b->h_ev[hb], b->stream), "step table event");
         b->h_cur ^= 1;
-        BCK(cudaEventRecord(b->ev0, b->stream), "timing event");
+        if (!launched) BCK(cudaEventRecord(b->ev0, b->stream), "timing event");
         BCK(cudaGraphLaunch(b->graph, b->stream), "graph launch");
-        BCK(cudaEventRecord(b->ev1, b->stream), "timing event");
-        BCK(cudaEventSynchronize(b->ev1), "graph sync");
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, b->ev0, b->ev1);
-        ms_total += ms;
+        launched = true;
         steps_done += adv;
     }
-    b->last_ms = ms_total;
+    if (launched) BCK(cudaEventRecord(b->ev1, b->stream), "timing event");
+    b->pending = launched;
+    b->last_ms = 0.0;
     b->last_steps = steps_done;
     return PF_OK;
+}
+
+// Waits for the steps of the last pf_batch_step_async; their device time is
+// then pf_batch_last_ms.
+int pf_batch_wait(pf_batch* b)
+{
+    if (!b) return berr(b, PF_E_ARG, "pf_batch_wait: bad argument");
+    if (!b->pending) return PF_OK;
+    BCK(cudaEventSynchronize(b->ev1), "batch wait");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    b->last_ms = ms;
+    b->pending = false;
+    return PF_OK;
+}
+
+int pf_batch_step(pf_batch* b, int n_steps)
+{
+    int rc = pf_batch_step_async(b, n_steps);
+    if (rc) return rc;
+    return pf_batch_wait(b);
 }
 
 double pf_batch_last_ms(const pf_batch* b) { return b ? b->last_ms : -1.0; }

@@ -13,7 +13,8 @@
 // each subroutine a C-ABI call.  With --fused the steps between output
 // events run as pf_step (same results).  Output events follow the E_R
 // counter (first at it = WriteFileD_timeCounter + 1): the diagnostics line,
-// and the Tecplot POINT file of saida.f90 in DIR/output/.  The progress line
+// and the Tecplot POINT file of saida.f90 in DIR/output/ (formatted and
+// written by a host thread while the loop steps on).  The progress line
 // of equacao_campo_fase.f90:174 is printed per sweep unless --quiet.
 #include <algorithm>
 #include <cctype>
@@ -26,6 +27,7 @@
 #include <sstream>
 #include <string>
 #include <vector>
+#include <thread>
 #include <sys/stat.h>
 #include "../../include/pf3d.h"
 #include "pf_fortfmt.h"
@@ -181,6 +183,37 @@ bool saida(const std::string& dir, const pf_grid& g, int it, float time, double 
     return true;
 }
 
+// Tecplot output off the time loop: the fields of an output event are copied
+// to the host, and a writer thread formats and writes them while the loop
+// steps on (one file in flight; the next event waits for it).
+class SaidaWriter {
+public:
+    SaidaWriter(std::string dir, pf_grid g) : dir_(std::move(dir)), g_(g) {}
+    ~SaidaWriter() { wait(); }
+    // takes the buffers (swapped out of the caller's vectors)
+    void submit(int it, float time, double TP, std::vector<double>& phi, std::vector<double>& c)
+    {
+        wait();
+        phi_.swap(phi);
+        c_.swap(c);
+        th_ = std::thread([this, it, time, TP]() {
+            if (!saida(dir_, g_, it, time, TP, phi_, c_)) ok_ = false;
+        });
+    }
+    void wait()
+    {
+        if (th_.joinable()) th_.join();
+    }
+    bool ok() const { return ok_; }
+
+private:
+    std::string dir_;
+    pf_grid g_;
+    std::vector<double> phi_, c_;
+    std::thread th_;
+    bool ok_ = true;
+};
+
 int fail(const char* what, pf_ctx* ctx, int rc)
 {
     std::fprintf(stderr, "%s failed (%d): %s\n", what, rc, pf_last_error(ctx));
@@ -234,6 +267,7 @@ int main(int argc, char** argv)
     CALL(pf_upload(ctx, PF_TOLD, T.data()), "upload TOLD");
     CALL(pf_upload(ctx, PF_DPP, dpp.data()), "upload DPP");
     if (output) mkdir((dir + "/output").c_str(), 0755);
+    SaidaWriter writer(dir, g);
 
     pf_state st;
     pf_get_state(ctx, &st);
@@ -280,9 +314,11 @@ int main(int argc, char** argv)
                             fort_e(dg[0], 14, 6).c_str(), fort_e(dg[1], 14, 6).c_str(), fort_e(dg[2], 14, 6).c_str(),
                             fort_e(dg[3], 14, 6).c_str(), fort_e(dg[4], 14, 6).c_str());
                 if (output) {
+                    phi.resize(n);
+                    c.resize(n);
                     CALL(pf_download(ctx, PF_PHASE_NEW, phi.data()), "download phase_field_new");
                     CALL(pf_download(ctx, PF_CONC_NEW, c.data()), "download conc_soluto_new");
-                    if (!saida(dir, g, (int)it, time, TP, phi, c)) std::fprintf(stderr, "saida: cannot write\n");
+                    writer.submit((int)it, time, TP, phi, c);
                 }
             }
             CALL(pf_swap(ctx), "swap");                                          // :200-226
@@ -296,11 +332,15 @@ int main(int argc, char** argv)
         }
     }
     CALL(pf_sync(ctx), "sync");
+    writer.wait();
+    if (!writer.ok()) std::fprintf(stderr, "saida: cannot write\n");
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     pf_get_state(ctx, &st);
     std::printf("Average Time/Step      : %.5f s\n", secs / std::max(1, st.it));
     // final state for a caller that inspects it: old fields after the swap
     if (output) {
+        phi.resize(n);
+        c.resize(n);
         CALL(pf_download(ctx, PF_PHASE_OLD, phi.data()), "download");
         CALL(pf_download(ctx, PF_CONC_OLD, c.data()), "download");
         FILE* f = std::fopen((dir + "/output/final_state.bin").c_str(), "wb");

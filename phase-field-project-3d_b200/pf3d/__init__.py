@@ -328,6 +328,15 @@ class Batch:
         self._chk(LIB.pf_batch_step(self._h, int(n)))
         return LIB.pf_batch_last_ms(self._h)
 
+    def step_async(self, n: int = 1):
+        """Queue up to n steps on the batch's stream and return at once."""
+        self._chk(LIB.pf_batch_step_async(self._h, int(n)))
+
+    def wait(self) -> float:
+        """Wait for the last step_async; returns its device ms."""
+        self._chk(LIB.pf_batch_wait(self._h))
+        return LIB.pf_batch_last_ms(self._h)
+
     def set_tile(self, tile_y: int, zchunk: int):
         self._chk(LIB.pf_batch_set_tile(self._h, tile_y, zchunk))
 

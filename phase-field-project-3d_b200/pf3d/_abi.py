@@ -113,6 +113,8 @@ SIGNATURES = [
     ("pf_batch_set_target", C.c_int, [_P, C.c_int, C.c_longlong]),
     ("pf_batch_get_state", C.c_int, [_P, C.c_int, C.POINTER(pf_state)]),
     ("pf_batch_step", C.c_int, [_P, C.c_int]),
+    ("pf_batch_step_async", C.c_int, [_P, C.c_int]),
+    ("pf_batch_wait", C.c_int, [_P]),
     ("pf_batch_last_ms", C.c_double, [_P]),
     ("pf_batch_set_tile", C.c_int, [_P, C.c_int, C.c_int]),
     ("pf_batch_set_paired", C.c_int, [_P, C.c_int]),

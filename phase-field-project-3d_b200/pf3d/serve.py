@@ -13,7 +13,8 @@ with probability 0.2 and parameters drawn as in the batching configuration.
 `Server` is the continuous-batching loop: requests that have arrived are
 admitted FIFO while they fit the device-memory budget (their state is
 created on the device), every admitted request advances together with the
-others in quanta of steps (one pf_batch_step per precision), and a request
+others in quanta of steps (one pf_batch_step_async per precision, the two
+precisions running at the same time on their own streams), and a request
 retires -- its diagnostics and its solid fraction and tip position
 (evaluated on the device) read back, its memory freed -- as soon as it has
 done its steps, which lets the next waiting requests in.  No field ever
@@ -172,12 +173,17 @@ class Server:
                     continue
                 if waiting:
                     raise RuntimeError("a request does not fit the device-memory budget on its own")
+            # both precisions' quanta run at the same time, each batch on its stream
+            stepped = []
             for prec, b in self.batches.items():
                 if self.active[prec]:
                     before = {s: b.state(s).it for s in self.active[prec]}
-                    device_ms += b.step(self.quantum)
-                    self.gcell_updates += sum(self.active[prec][s].cells * (b.state(s).it - before[s])
-                                              for s in self.active[prec]) / 1e9
+                    b.step_async(self.quantum)
+                    stepped.append((prec, b, before))
+            for prec, b, before in stepped:
+                device_ms += b.wait()
+                self.gcell_updates += sum(self.active[prec][s].cells * (b.state(s).it - before[s])
+                                          for s in self.active[prec]) / 1e9
             self._retire(clock() - t0, done)
             if on_quantum:
                 on_quantum(self, done, waiting)

@@ -50,6 +50,30 @@ def test_batch_equals_alone(gpu, prec):
                 assert np.array_equal(got[k], want[k]), (s, k)
 
 
+def test_async_batches_run_together(gpu):
+    """Two batches (FP64 and FP32) queued with step_async run on their own
+    streams at the same time; after wait() every domain has its alone bits,
+    and steps spanning several graphs (more than 8) keep them too."""
+    cases = [case(40, 30, 36), case(28, 44, 30, T0=919.0)]
+    with pf3d.Batch(pf3d.PF_FP64) as b64, pf3d.Batch(pf3d.PF_FP32) as b32:
+        slots = {}
+        for b in (b64, b32):
+            for i, (g, p, st) in enumerate(cases):
+                s = b.add(g, p)
+                b.load_state(s, st)
+                slots[(id(b), i)] = s
+        for n in (5, 19):
+            b64.step_async(n)
+            b32.step_async(n)
+            assert b64.wait() > 0 and b32.wait() > 0
+        for b, prec in ((b64, pf3d.PF_FP64), (b32, pf3d.PF_FP32)):
+            for i, (g, p, st) in enumerate(cases):
+                want, _ = alone(g, p, st, prec, 24)
+                got = b.fields(slots[(id(b), i)])
+                for k in want:
+                    assert np.array_equal(got[k], want[k]), (prec, i, k)
+
+
 def test_paired_batch_equals_alone(gpu):
     """FP32 batch with two cells per thread: every domain keeps its alone bits
     (domains big enough to have interior tiles, and small ragged ones)."""
