@@ -30,8 +30,8 @@ struct F2 {
     }
     __device__ __forceinline__ explicit F2(float a) { asm("mov.b64 %0, {%1, %1};" : "=l"(v) : "f"(a)); }
     __device__ __forceinline__ F2(float a, float b) { asm("mov.b64 %0, {%1, %2};" : "=l"(v) : "f"(a), "f"(b)); }
-    __device__ __forceinline__ float x() const { float a, b; asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); (void)b; return a; }
-    __device__ __forceinline__ float y() const { float a, b; asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); (void)a; return b; }
+    __device__ __forceinline__ float x() const { float a; asm("{ .reg .f32 t; mov.b64 {%0, t}, %1; }" : "=f"(a) : "l"(v)); return a; }
+    __device__ __forceinline__ float y() const { float b; asm("{ .reg .f32 t; mov.b64 {t, %0}, %1; }" : "=f"(b) : "l"(v)); return b; }
     __device__ __forceinline__ float lane(int i) const { return i ? y() : x(); }
 };
 __device__ __forceinline__ F2 operator+(F2 a, F2 b) { return F2(__fadd_rn(a.x(), b.x()), __fadd_rn(a.y(), b.y())); }
