@@ -300,9 +300,12 @@ __device__ __forceinline__ Node<T> aniso_node(T gx, T gy, T gz, const KC<T>& c)
         const T rq = Ar<T>::rcp(Q * Q);
         n.eps = c.E0 * fmadd(c.DE, fmadd((T)4 * S4, rq, (T)-3), (T)1);
         const T f = c.K * n.eps * rq;
-        n.exy = f * ux * uy * (ux2 - uy2);
-        n.eyz = f * uy * uz * (uy2 - uz2);
-        n.ezx = f * uz * ux * (uz2 - ux2);
+        // every product that feeds a sum is an explicit multiply-add in the
+        // FP32 form: nothing is left for a compiler to contract, so the lane
+        // pairs may issue packed f32x2 products and sums (pf3d_pair.cuh)
+        n.exy = f * ux * uy * fmadd(ux, ux, -uy2);
+        n.eyz = f * uy * uz * fmadd(uy, uy, -uz2);
+        n.ezx = f * uz * ux * fmadd(uz, uz, -ux2);
     }
     (void)gx2; (void)gy2; (void)gz2;
     return n;
@@ -378,22 +381,39 @@ __device__ __forceinline__ T phase_ppnew(const Nbr<T>& p, const Node<T>& E, cons
                             fmadd(B.ezx, (p.PWB - p.PEB) + (p.PW - p.PE), E.ezx * ((p.PEB - p.PET) + (p.PB - p.PT)))));
         AA = fmadd(c.cxy, Cxy, fmadd(c.cyz, Cyz, fmadd(c.czx, Czx, AA)));
         const T q = one - PP;
-        T g_linha = two * PP * q * (one - two * PP);
-        T h_linha, h;
-        if (c.hq == 1) {
-            h_linha = (T)30 * PP * PP * q * q;
-            h = PP * PP * PP * ((T)10 - (T)15 * PP + (T)6 * PP * PP);
+        T g_linha, h_linha, h;
+        if constexpr (IsF64<T>::value) {
+            g_linha = two * PP * q * (one - two * PP);
+            if (c.hq == 1) {
+                h_linha = (T)30 * PP * PP * q * q;
+                h = PP * PP * PP * ((T)10 - (T)15 * PP + (T)6 * PP * PP);
+            } else {
+                h_linha = (T)6 * PP * q;
+                h = PP * PP * ((T)3 - two * PP);
+            }
         } else {
-            h_linha = (T)6 * PP * q;
-            h = PP * PP * ((T)3 - two * PP);
+            // FP32: products feeding sums as explicit multiply-adds
+            g_linha = two * PP * q * fmadd(-two, PP, one);
+            if (c.hq == 1) {
+                h_linha = (T)30 * PP * PP * q * q;
+                h = PP * PP * PP * fmadd((T)6 * PP, PP, fmadd((T)-15, PP, (T)10));
+            } else {
+                h_linha = (T)6 * PP * q;
+                h = PP * PP * fmadd(-two, PP, (T)3);
+            }
         }
         T den = fmadd(-c.omKe, h, one);
         // (1-CLP)/(1-CSP) = (den - c)/(den - Ke c); the constant factor is in Lc
         T lg = Ar<T>::lg(vabs(Ar<T>::div(den - CPP, fmadd(-c.Ke, CPP, den)))) + c.Lc;
         T GG = fmadd(c.RTV * h_linha, lg, -(c.W0 * g_linha));
         T pp2q2 = PP * PP * q * q * c.AAA16;
-        T ruidos = (c.rt == 0) ? (T)ran * pp2q2 : fmadd(two, (T)ran, -one) * pp2q2;
-        return fmadd(c.M0dt, AA + GG, PP + ruidos);
+        if constexpr (IsF64<T>::value) {
+            T ruidos = (c.rt == 0) ? (T)ran * pp2q2 : fmadd(two, (T)ran, -one) * pp2q2;
+            return fmadd(c.M0dt, AA + GG, PP + ruidos);
+        } else {
+            const T r = (c.rt == 0) ? (T)ran : fmadd(two, (T)ran, -one);
+            return fmadd(c.M0dt, AA + GG, fmadd(r, pp2q2, PP));
+        }
     }
 }
 
@@ -432,12 +452,29 @@ __device__ __forceinline__ SolNode<T> sol_node(T P, T C, const KC<T>& c)
         T CL = C / den;
         n.br = (one - h) * CL * (one - CL) + h * CS * (one - CS);
         n.mu = log(CL / (one - CL));
-    } else {
+    } else if constexpr (IsF64<T>::value) {
         T den = fmadd(-c.omKe, h, one);
         T CL = C * Ar<T>::rcp(den);
         T CS = c.Ke * CL;
         n.br = fmadd((one - h) * CL, one - CL, h * CS * (one - CS));
         n.mu = Ar<T>::lg(Ar<T>::div(C, den - C));   // CL/(1-CL) = C/(den-C)
+    } else {
+        // FP32: h = a*b with 1-h, 1-CL and 1-CS as explicit multiply-adds
+        T a, b;
+        if (c.hq == 1) {
+            a = P * P * P;
+            b = fmadd((T)6 * P, P, fmadd((T)-15, P, (T)10));
+        } else {
+            a = P * P;
+            b = fmadd((T)-2, P, (T)3);
+        }
+        const T hf = a * b, omh = fmadd(-a, b, one);
+        const T den = fmadd(-c.omKe, hf, one);
+        const T rd = Ar<T>::rcp(den);
+        const T CL = C * rd, CS = c.Ke * CL;
+        n.br = fmadd(omh * CL, fmadd(-C, rd, one), hf * CS * fmadd(-c.Ke, CL, one));
+        n.mu = Ar<T>::lg(Ar<T>::div(C, den - C));
+        (void)h;
     }
     return n;
 }

@@ -1,15 +1,15 @@
 // pf3d_pair.cuh -- lane-pair arithmetic: two cells per thread.
 //
-// F2 holds two floats in one 64-bit register pair.  Its explicit multiply-add
-// is Blackwell's packed fma.rn.f32x2 (sm_100a): one instruction, the same
-// IEEE fused operation on both cells.  Products, sums and differences stay
-// one scalar instruction per lane: ptxas contracts a packed mul.rn.f32x2 that
-// feeds a packed add.rn.f32x2 into a packed fma even under --fmad=false
-// (measured on B200: 15 % of random operands round differently), which would
-// break the rule that nothing is contracted unless asked for.  D2 holds two
-// doubles and does each operation once per lane.  Every operation is the
-// scalar one per lane, so a cell computed in a pair has the bits it has when
-// computed alone.
+// F2 holds two floats in one 64-bit register pair and maps add, sub, mul and
+// fma onto Blackwell's packed FP32 instructions (add/sub/mul/fma.rn.f32x2,
+// sm_100a): one instruction, the same IEEE operation on both cells.  ptxas
+// contracts a packed mul.rn.f32x2 that feeds a packed add.rn.f32x2 into a
+// packed fma even under --fmad=false (measured on B200: 15 % of random
+// operands then round differently), so the FP32 fast form that runs on F2
+// writes every product that feeds a sum as an explicit fmadd: nothing is left
+// to contract, and the packed and the scalar kernels agree bit for bit
+// (tests/test_paired_gpu.py).  D2 holds two doubles and does each operation
+// once per lane.
 #pragma once
 #include <cstdint>
 #include <cstring>
@@ -34,9 +34,9 @@ struct F2 {
     __device__ __forceinline__ float y() const { float b; asm("{ .reg .f32 t; mov.b64 {t, %0}, %1; }" : "=f"(b) : "l"(v)); return b; }
     __device__ __forceinline__ float lane(int i) const { return i ? y() : x(); }
 };
-__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return F2(__fadd_rn(a.x(), b.x()), __fadd_rn(a.y(), b.y())); }
-__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return F2(__fsub_rn(a.x(), b.x()), __fsub_rn(a.y(), b.y())); }
-__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return F2(__fmul_rn(a.x(), b.x()), __fmul_rn(a.y(), b.y())); }
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { F2 r; asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v)); return r; }
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) { F2 r; asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v)); return r; }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { F2 r; asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v)); return r; }
 // exact negation: flip both sign bits
 __device__ __forceinline__ F2 operator-(F2 a) { F2 r; r.v = a.v ^ 0x8000000080000000ull; return r; }
 __device__ __forceinline__ F2 fmadd(F2 a, F2 b, F2 c) { F2 r; asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v)); return r; }
