@@ -63,6 +63,71 @@ struct FusedOcc {
 __device__ __forceinline__ int add6(int a, int k) { int t = a + k; return t >= 6 ? t - 6 : t; }
 __device__ __forceinline__ int add3(int a, int k) { int t = a + k; return t >= 3 ? t - 3 : t; }
 
+// One cell of a boundary tile or plane, shared by the one-cell and the
+// paired kernels: the heat update (TNEW <- TOLD outside 2..N-1), the phase
+// sweep with the closed-form decoration of equacao_campo_fase.f90:151-167
+// (the source cell writes its value to all its preimages) and the solute
+// update with the face copies of concentracao_soluto.f90:116-124.  phase(),
+// heat() and solute() evaluate the cell's arithmetic; [xl, xh] and [yl, yh]
+// are the cell's x and y preimage ranges (fpre_range).
+template <typename T, bool HEAT, bool DPPW, bool SOL, typename PhaseF, typename HeatF, typename SolF>
+__device__ __forceinline__ void boundary_cell(int x, int y, int z, int nx, int ny, int nz, long long px, long long pl,
+                                              long long id, T PPc, T cpp, T told, int xl, int xh, int yl, int yh,
+                                              T* __restrict__ phi_out, T* __restrict__ dpp, T* __restrict__ c_out,
+                                              T* __restrict__ T_new, PhaseF phase, HeatF heat, SolF solute)
+{
+    const bool xs_src = x >= 1 && x <= nx - 2, ys_src = y >= 1 && y <= ny - 2;
+    const bool xs_int = x >= 2 && x <= nx - 3, ys_int = y >= 2 && y <= ny - 3;
+    const bool single_xy = x >= 3 && x <= nx - 4 && y >= 3 && y <= ny - 4;
+    const bool zin = z >= 1 && z <= nz - 2;
+
+    // ---- temperatura ----
+    if (HEAT) T_new[id] = (xs_src && ys_src && zin) ? heat() : told;
+
+    // ---- phase sweep ----
+    if (xs_src && ys_src && zin) {
+        T U;
+        if (xs_int && ys_int && z >= 2 && z <= nz - 3) {
+            const T ppn = phase();
+            if (DPPW) dpp[id] = ppn - PPc;
+            U = clamp01(ppn);
+        } else {
+            U = PPc;
+        }
+        if (single_xy && z >= 3 && z <= nz - 4) {
+            phi_out[id] = U;   // its only preimage is itself
+        } else {
+            int zl, zh;
+            fpre_range(z, nz, &zl, &zh);
+            for (int zz = zl; zz <= zh; ++zz)
+                for (int yy = yl; yy <= yh; ++yy)
+                    for (int xx = xl; xx <= xh; ++xx)
+                        phi_out[(long long)xx + (long long)yy * px + (long long)zz * pl] = U;
+        }
+    }
+
+    // ---- solute ----
+    if (SOL) {
+        const bool inner = xs_src && ys_src && zin;
+        const bool feeds = inner || z == 1 || z == nz - 2 || (zin && (x == 1 || x == nx - 2));
+        if (feeds) {
+            T Uc;
+            if (inner) {
+                Uc = solute();
+                c_out[id] = Uc;
+            } else {
+                Uc = cpp;
+            }
+            if (z == 1) c_out[id - pl] = Uc;
+            if (z == nz - 2) c_out[id + pl] = Uc;
+            if (zin && x == 1) c_out[id - 1] = Uc;
+            if (zin && x == nx - 2) c_out[id + 1] = Uc;
+            if (zin && xs_src && y == 1) c_out[id - px] = Uc;
+            if (zin && xs_src && y == ny - 2) c_out[id + px] = Uc;
+        }
+    }
+}
+
 // One 32 x TY x zchunk tile (tile coordinates bx, by, bz) of one domain.
 // Ends with a CTA-wide barrier, so the caller may reuse the shared memory.
 template <typename T, int TY, bool HEAT, bool DPPW, bool SOL, bool SMOOTH>
@@ -196,8 +261,6 @@ __device__ __forceinline__ void fused_tile(const DomainDesc& d, const KC<T>& c, 
     const int fx = tx + 2, fy = ty + 2;   // own cell in the phase tile
     const int nlx = tx + 1, nly = ty + 1; // own cell in the node tile
     const bool xs_src = x >= 1 && x <= nx - 2, ys_src = y >= 1 && y <= ny - 2;
-    const bool xs_int = x >= 2 && x <= nx - 3, ys_int = y >= 2 && y <= ny - 3;
-    const bool single_xy = x >= 3 && x <= nx - 4 && y >= 3 && y <= ny - 4;
     // CTA-uniform: every column of the tile is in [3, N-4] in x and y
     const bool tile_int = x0 >= 3 && x0 + TX + 3 <= nx && y0 >= 3 && y0 + TY + 3 <= ny;
     int xl = 0, xh = -1, yl = 0, yh = -1;
@@ -308,53 +371,10 @@ __device__ __forceinline__ void fused_tile(const DomainDesc& d, const KC<T>& c, 
             if (SOL) c_out[id] = solute_cell(PPc, cpp);
         } else if (own) {
             const T PPc = p0[fy][fx];
-            const bool zin = z >= 1 && z <= nz - 2;
-
-            // ---- temperatura ----
-            if (HEAT) T_new[id] = (xs_src && ys_src && zin) ? heat_cell(PPc, dppv) : told;
-
-            // ---- phase sweep ----
-            if (xs_src && ys_src && zin) {
-                T U;
-                if (xs_int && ys_int && z >= 2 && z <= nz - 3) {
-                    const T ppn = phase_cell(PPc, cpp, z);
-                    if (DPPW) dpp[id] = ppn - PPc;
-                    U = clamp01(ppn);
-                } else {
-                    U = PPc;
-                }
-                if (single_xy && z >= 3 && z <= nz - 4) {
-                    phi_out[id] = U;   // its only preimage is itself
-                } else {
-                    int zl, zh;
-                    fpre_range(z, nz, &zl, &zh);
-                    for (int zz = zl; zz <= zh; ++zz)
-                        for (int yy = yl; yy <= yh; ++yy)
-                            for (int xx = xl; xx <= xh; ++xx)
-                                phi_out[(long long)xx + (long long)yy * px + (long long)zz * pl] = U;
-                }
-            }
-
-            // ---- solute ----
-            if (SOL) {
-                const bool inner = xs_src && ys_src && zin;
-                const bool feeds = inner || z == 1 || z == nz - 2 || (zin && (x == 1 || x == nx - 2));
-                if (feeds) {
-                    T Uc;
-                    if (inner) {
-                        Uc = solute_cell(PPc, cpp);
-                        c_out[id] = Uc;
-                    } else {
-                        Uc = cpp;
-                    }
-                    if (z == 1) c_out[id - pl] = Uc;
-                    if (z == nz - 2) c_out[id + pl] = Uc;
-                    if (zin && x == 1) c_out[id - 1] = Uc;
-                    if (zin && x == nx - 2) c_out[id + 1] = Uc;
-                    if (zin && xs_src && y == 1) c_out[id - px] = Uc;
-                    if (zin && xs_src && y == ny - 2) c_out[id + px] = Uc;
-                }
-            }
+            boundary_cell<T, HEAT, DPPW, SOL>(
+                x, y, z, nx, ny, nz, px, pl, id, PPc, cpp, told, xl, xh, yl, yh, phi_out, dpp, c_out, T_new,
+                [&]() { return phase_cell(PPc, cpp, z); }, [&]() { return heat_cell(PPc, dppv); },
+                [&]() { return solute_cell(PPc, cpp); });
         }
         if (SOL) { cpi = cqi; cpr = cqr; }
         cp_async_wait_prev();   // plane z+3 (needed next) has landed; z+4 may be in flight

@@ -208,7 +208,7 @@ __device__ __forceinline__ void fused_tile_pair(const DomainDesc& d, const KC<S>
 
     const int fx = tx + 2, nlx = tx + 1;
     const int fyv[2] = {ty + 2, ty + 2 + TYH}, nlyv[2] = {ty + 1, ty + 1 + TYH};
-    const bool xs_src = x >= 1 && x <= nx - 2, xs_int = x >= 2 && x <= nx - 3;
+    const bool xs_src = x >= 1 && x <= nx - 2;
     const bool tile_int = x0 >= 3 && x0 + TX + 3 <= nx && y0 >= 3 && y0 + TY + 3 <= ny;
     int xl = 0, xh = -1;
     if ((own[0] || own[1]) && xs_src) fpre_range(x, nx, &xl, &xh);
@@ -375,56 +375,17 @@ __device__ __forceinline__ void fused_tile_pair(const DomainDesc& d, const KC<S>
             }
         } else {
             // boundary tiles and planes: fused_tile's scalar path, lane by lane
-            int zl = 0, zh = -1;
-            fpre_range(z, nz, &zl, &zh);
             for (int l = 0; l < 2; ++l) {
                 if (!own[l]) continue;
                 const int y = yv[l];
                 const long long id = col[l] + zoff;
                 const S PPc = p0[fyv[l]][fx];
-                const bool zin = z >= 1 && z <= nz - 2;
-                const bool ys_src = y >= 1 && y <= ny - 2, ys_int = y >= 2 && y <= ny - 3;
-                const bool single_xy = x >= 3 && x <= nx - 4 && y >= 3 && y <= ny - 4;
-                if (HEAT) T_new[id] = (xs_src && ys_src && zin) ? heat_cell_s(l, id, PPc) : told[l];
-                if (xs_src && ys_src && zin) {
-                    S U;
-                    if (xs_int && ys_int && z >= 2 && z <= nz - 3) {
-                        const S ppn = phase_cell_s(l, id);
-                        if (DPPW) dpp[id] = ppn - PPc;
-                        U = clamp01(ppn);
-                    } else {
-                        U = PPc;
-                    }
-                    if (single_xy && z >= 3 && z <= nz - 4) {
-                        phi_out[id] = U;
-                    } else {
-                        int yl_, yh_;
-                        fpre_range(y, ny, &yl_, &yh_);
-                        for (int zz = zl; zz <= zh; ++zz)
-                            for (int yy = yl_; yy <= yh_; ++yy)
-                                for (int xx = xl; xx <= xh; ++xx)
-                                    phi_out[(long long)xx + (long long)yy * px + (long long)zz * pl] = U;
-                    }
-                }
-                if (SOL) {
-                    const bool inner = xs_src && ys_src && zin;
-                    const bool feeds = inner || z == 1 || z == nz - 2 || (zin && (x == 1 || x == nx - 2));
-                    if (feeds) {
-                        S Uc;
-                        if (inner) {
-                            Uc = solute_cell_s(l, PPc);
-                            c_out[id] = Uc;
-                        } else {
-                            Uc = cpp[l];
-                        }
-                        if (z == 1) c_out[id - pl] = Uc;
-                        if (z == nz - 2) c_out[id + pl] = Uc;
-                        if (zin && x == 1) c_out[id - 1] = Uc;
-                        if (zin && x == nx - 2) c_out[id + 1] = Uc;
-                        if (zin && xs_src && y == 1) c_out[id - px] = Uc;
-                        if (zin && xs_src && y == ny - 2) c_out[id + px] = Uc;
-                    }
-                }
+                int yl_ = 0, yh_ = -1;
+                if (y >= 1 && y <= ny - 2) fpre_range(y, ny, &yl_, &yh_);
+                boundary_cell<S, HEAT, DPPW, SOL>(
+                    x, y, z, nx, ny, nz, px, pl, id, PPc, cpp[l], told[l], xl, xh, yl_, yh_, phi_out, dpp, c_out,
+                    T_new, [&]() { return phase_cell_s(l, id); }, [&]() { return heat_cell_s(l, id, PPc); },
+                    [&]() { return solute_cell_s(l, PPc); });
             }
         }
         if (SOL) {
