@@ -366,6 +366,14 @@ int pf_karma_step(pf_karma* k, int n_steps);
 int pf_karma_tip(pf_karma* k, int* tip_x, int* tip_d);
 int pf_karma_sync(pf_karma* k);
 
+/* ---- self-check of the fast form's own FP64 logarithm ------------------
+   The fused FP64 kernels take log(CL/(1-CL)) and log|...| of
+   phase_body.inc / soluto_body.inc with this library's logarithm (atanh
+   series with argument reduction) instead of the CUDA library's.  This
+   evaluates both on the device for n host values: own[i] = the fused
+   kernels' log(x[i]), lib[i] = CUDA's log(x[i]).  No reference routine.   */
+int pf_math_log(const double* x, long long n, double* own, double* lib);
+
 #ifdef __cplusplus
 }
 #endif

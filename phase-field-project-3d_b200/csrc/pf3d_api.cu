@@ -737,4 +737,20 @@ int pf_kernel_times(pf_ctx* ctx, long* n_first, double* ms_first, long* n_last, 
     return PF_OK;
 }
 
+int pf_math_log(const double* x, long long n, double* own, double* lib)
+{
+    if (n < 0 || (n > 0 && (!x || !own || !lib)) || n > (1LL << 28))
+        return ctx_err(nullptr, PF_E_ARG, "pf_math_log: bad argument");
+    if (n == 0) return PF_OK;
+    const size_t bytes = (size_t)n * sizeof(double);
+    double* d = nullptr;
+    if (int rc = cuda_check(nullptr, cudaMalloc(&d, 3 * bytes), "pf_math_log alloc")) return rc;
+    cudaError_t e = cudaMemcpy(d, x, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launch_math_log(d, d + n, d + 2 * n, n, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(own, d + n, bytes, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(lib, d + 2 * n, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return cuda_check(nullptr, e, "pf_math_log");
+}
+
 }  // extern "C"

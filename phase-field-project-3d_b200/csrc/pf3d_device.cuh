@@ -145,12 +145,64 @@ __device__ __forceinline__ double rcp_nr(double b)
     return __fma_rn(y, e, y);
 }
 
+// Natural logarithm in FP64 for the fast form -- this library's own, written
+// from the mathematics, not the CUDA library's: x = 2^k m with m in
+// [sqrt(1/2), sqrt(2)), f = m - 1 (exact, Sterbenz), and
+//     log x = k ln2 + 2 atanh(s) = k ln2 + 2s + 2s z P(z),
+//     s = f/(2 + f),  |s| <= 0.17158,  z = s^2 <= 0.029438,
+// where P(z) = (atanh(sqrt z)/sqrt z - 1)/z = 1/3 + z/5 + z^2/7 + ... (the
+// Taylor series of atanh) is replaced by its degree-6 Chebyshev interpolant
+// on [0, 0.029441] (Lanczos economization; coefficients and their error from
+// log_coeffs.py: |P6 - P| <= 1.6e-16, i.e. below 5e-18 of log x after the
+// factor 2s z).  The reduction works on the high word: adding
+// 0x3ff00000 - 0x3fe6a09e (0x3fe6a09e = high word of sqrt(1/2)) carries into
+// the exponent field exactly when the mantissa is at or above sqrt(2)'s, so k
+// and m come out of integer operations with no compare.  s is carried as
+// s + sl: the rounding error of 2 + f (Fast2Sum, Dekker 1971) and the residual
+// of the quotient (one Newton correction, Markstein 1990) go into sl, which
+// joins the low-order sum.  ln2 is split into a head with the low 32 mantissa
+// bits zero, so k ln2_hi is exact, and a tail.  Within 1 ulp of log x
+// (pf_math_log, tests).  Zero, negative, subnormal, infinite and NaN
+// arguments (one unsigned compare on the high word) call the CUDA library's
+// log out of line, so nothing of it is evaluated on the common path.
+static __device__ __noinline__ double log_special(double x) { return log(x); }
+__device__ __forceinline__ double pf_log(double x)
+{
+    int hi = __double2hiint(x);
+    const int lo = __double2loint(x);
+    if ((unsigned)(hi - 0x00100000) >= 0x7fe00000u) return log_special(x);
+    hi += 0x3ff00000 - 0x3fe6a09e;
+    const int k = (hi >> 20) - 0x3ff;
+    const double m = __hiloint2double((hi & 0x000fffff) + 0x3fe6a09e, lo);   // [sqrt(1/2), sqrt(2))
+    const double f = m - 1.0;                      // exact
+    const double d = 2.0 + f;
+    const double derr = f - (d - 2.0);             // 2 + f = d + derr exactly
+    const double rc = rcp_nr(d);
+    const double s = f * rc;
+    const double e = __fma_rn(-s, derr, __fma_rn(-s, d, f));   // f - s (d + derr)
+    const double sl = e * rc;                      // f/(2 + f) = s + sl
+    const double z = s * s;
+    double p = 0.07308292712444311;
+    p = __fma_rn(p, z, 0.07665855309105386);
+    p = __fma_rn(p, z, 0.09091444727837474);
+    p = __fma_rn(p, z, 0.11111105565129939);
+    p = __fma_rn(p, z, 0.14285714313001635);
+    p = __fma_rn(p, z, 0.19999999999949722);
+    p = __fma_rn(p, z, 0.3333333333333335);
+    const double t = 2.0 * s;                      // exact
+    const double lo_sum = __fma_rn(t * z, p, sl + sl);   // 2 atanh(s) - t
+    const double kd = (double)k;
+    const double ln2_hi = 0.6931467056274414;      // 0x3fe62e4200000000
+    const double ln2_lo = 4.7493250390316726e-07;  // ln2 - ln2_hi
+    return __fma_rn(kd, ln2_hi, __fma_rn(kd, ln2_lo, lo_sum) + t);
+}
+
 // Arithmetic of the fast form (the reference form uses plain / and log).
 template <typename T> struct Ar;
 template <> struct Ar<double> {
     static __device__ __forceinline__ double rcp(double x) { return rcp_nr(x); }
     static __device__ __forceinline__ double div(double a, double b) { return a * rcp_nr(b); }
-    static __device__ __forceinline__ double lg(double x) { return log(x); }
+    static __device__ __forceinline__ double lg(double x) { return pf_log(x); }
 };
 template <> struct Ar<float> {
     static __device__ __forceinline__ float rcp(float x) { return __fdividef(1.0f, x); }
@@ -198,7 +250,7 @@ template <> struct Ar<F2> {
 template <> struct Ar<D2> {
     static __device__ __forceinline__ D2 rcp(D2 x) { return D2(rcp_nr(x.a), rcp_nr(x.b)); }
     static __device__ __forceinline__ D2 div(D2 a, D2 b) { return D2(a.a * rcp_nr(b.a), a.b * rcp_nr(b.b)); }
-    static __device__ __forceinline__ D2 lg(D2 x) { return D2(log(x.a), log(x.b)); }
+    static __device__ __forceinline__ D2 lg(D2 x) { return D2(pf_log(x.a), pf_log(x.b)); }
 };
 
 // Explicit multiply-add.  Every translation unit is built without automatic

@@ -11,4 +11,24 @@ template cudaError_t launch_fused_batch<double>(const BatchDomain*, const BatchS
 template cudaError_t launch_fused_first_pair<double>(const DomainDesc&, const StepArgs&, const Fields&, bool, int, cudaStream_t);
 template cudaError_t launch_fused_last_pair<double>(const DomainDesc&, const StepArgs&, const Fields&, int, cudaStream_t);
 template cudaError_t launch_fused_batch_pair<double>(const BatchDomain*, const BatchStep*, const BatchItem*, const int*, int, bool, int, int, cudaStream_t);
+
+__global__ void k_math_log(const double* __restrict__ x, double* __restrict__ own, double* __restrict__ lib,
+                           long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double v = x[i];
+        own[i] = Ar<double>::lg(v);
+        lib[i] = log(v);
+    }
+}
+
+cudaError_t launch_math_log(const double* x, double* own, double* lib, long long n, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    const long long want = (n + 255) / 256;
+    const int grid = (int)(want < 148 * 8 ? want : 148 * 8);
+    k_math_log<<<grid, 256, 0, st>>>(x, own, lib, n);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
+}
 }  // namespace pf3d

@@ -96,4 +96,8 @@ template <typename T> cudaError_t launch_convert_in(const DomainDesc& d, const d
 template <typename T> cudaError_t launch_convert_out(const DomainDesc& d, const void* src, double* stage, long long z0,
                                                      long long nz, cudaStream_t st);
 
+// Self-check of the fast form's FP64 logarithm: own[i] = pf_log(x[i]),
+// lib[i] = the CUDA library's log(x[i]).
+cudaError_t launch_math_log(const double* x, double* own, double* lib, long long n, cudaStream_t st);
+
 }  // namespace pf3d

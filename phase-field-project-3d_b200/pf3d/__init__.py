@@ -45,6 +45,16 @@ def auxiliar_scalar(p: pf_params, E0: float, W0: float, TP: float, Cs_eq: float,
     return M0.value
 
 
+def math_log(x) -> "tuple[np.ndarray, np.ndarray]":
+    """The fused FP64 kernels' own logarithm and CUDA's log, both evaluated on
+    the device for the values x (self-check of the fast form's arithmetic)."""
+    x = np.ascontiguousarray(x, dtype=np.float64).ravel()
+    own = np.empty_like(x)
+    lib = np.empty_like(x)
+    check(LIB.pf_math_log(_dptr(x), x.size, _dptr(own), _dptr(lib)))
+    return own, lib
+
+
 class Domain:
     """One device-resident domain (a pf_ctx)."""
 

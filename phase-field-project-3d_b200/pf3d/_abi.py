@@ -137,6 +137,7 @@ SIGNATURES = [
     ("pf_karma_sync", C.c_int, [_P]),
     ("pf_diagnosticos_noalloc", C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                           C.c_double, C.c_double, C.c_double, C.c_double, _P, _D]),
+    ("pf_math_log", C.c_int, [_P, C.c_longlong, _P, _P]),
 ]
 
 
