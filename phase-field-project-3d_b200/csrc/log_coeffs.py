@@ -25,19 +25,25 @@ def P(z):
     return (mp.atanh(r) / r - 1) / z
 
 
-def main(degree=6):
+def coefficients(degree=6, grid=4000):
+    """(coefficients highest degree first, max |P6 - P| on the grid)."""
     poly, _ = mp.chebyfit(P, [0, Z_MAX], degree + 1, error=True)
-    coeffs = [float(c) for c in poly]          # highest degree first (Horner order)
+    coeffs = [float(c) for c in poly]          # Horner order
     worst = mp.mpf(0)
-    for i in range(4001):
-        z = Z_MAX * i / 4000
+    for i in range(grid + 1):
+        z = Z_MAX * i / grid
         v = mp.mpf(0)
         for c in coeffs:
             v = v * z + mp.mpf(c)
         worst = max(worst, abs(v - P(z)))
+    return coeffs, float(worst)
+
+
+def main():
+    coeffs, worst = coefficients()
     for c in coeffs:
         print(repr(c))
-    print("max |P6 - P| = %.3g, in log x at most %.3g" % (float(worst), float(worst * Z_MAX)))
+    print("max |P6 - P| = %.3g, in log x at most %.3g" % (worst, worst * float(Z_MAX)))
 
 
 if __name__ == "__main__":
