@@ -23,7 +23,7 @@ from ._abi import (LIB, check, pf_grid, pf_params, pf_derived, pf_state, PFError
 from .deck import run6_params, params_copy, grid, read_entrada, WORKLOADS, Workload
 
 __all__ = ["Domain", "PFError", "run6_params", "params_copy", "grid", "read_entrada", "WORKLOADS", "Workload",
-           "w0_e0", "auxiliar_scalar", "FIELDS", "PF_FP64", "PF_FP32"]
+           "w0_e0", "auxiliar_scalar", "math_log", "FIELDS", "PF_FP64", "PF_FP32"]
 
 FIELDS = {n: q for q, n in enumerate(FIELD_NAMES)}
 FIELDS.update({"phi_old": 0, "phi_new": 1, "c_old": 2, "c_new": 3, "T_old": 4, "T_new": 5, "dpp": 6})

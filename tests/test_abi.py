@@ -64,6 +64,17 @@ def test_rejects_small_grid():
     assert e.value.code == _abi.PF_E_ARG
 
 
+def test_math_log_argument_checks():
+    # checked before any CUDA call, so this runs without a device
+    x = np.ones(4)
+    y = np.empty(4)
+    ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+    assert _abi.LIB.pf_math_log(ptr(x), -1, ptr(y), ptr(y)) == _abi.PF_E_ARG
+    assert _abi.LIB.pf_math_log(None, 4, ptr(y), ptr(y)) == _abi.PF_E_ARG
+    assert _abi.LIB.pf_math_log(ptr(x), 1 << 29, ptr(y), ptr(y)) == _abi.PF_E_ARG
+    assert _abi.LIB.pf_math_log(None, 0, None, None) == _abi.PF_OK
+
+
 def test_ctx_bytes():
     g = deck.grid(512, 512, 1024, 0.5e-6)
     b64 = _abi.LIB.pf_ctx_bytes(C.byref(g), 64)
