@@ -111,12 +111,19 @@ def ctx_bytes(job: Job) -> int:
 
 
 class Server:
-    """Continuous batching of solidification requests on one GPU."""
+    """Continuous batching of solidification requests on one GPU.
 
-    def __init__(self, budget_bytes: float = 150e9, quantum: int = 8, max_slots: int = 4096):
+    `batch_factory(precision, budget, max_slots)` makes the per-precision
+    batches (pf3d.Batch) and `bytes_of(job)` sizes a request's device memory
+    (pf_ctx_bytes); both are parameters so that the scheduling can be driven
+    by stand-ins on a machine without a GPU."""
+
+    def __init__(self, budget_bytes: float = 150e9, quantum: int = 8, max_slots: int = 4096,
+                 batch_factory=Batch, bytes_of=None):
         self.budget = int(budget_bytes)
         self.quantum = quantum
-        self.batches = {PF_FP32: Batch(PF_FP32, 0, max_slots), PF_FP64: Batch(PF_FP64, 0, max_slots)}
+        self.bytes_of = bytes_of if bytes_of is not None else ctx_bytes
+        self.batches = {PF_FP32: batch_factory(PF_FP32, 0, max_slots), PF_FP64: batch_factory(PF_FP64, 0, max_slots)}
         self.used = 0
         self.active: dict = {PF_FP32: {}, PF_FP64: {}}   # slot -> job
         self.gcell_updates = 0.0
@@ -126,7 +133,7 @@ class Server:
             b.close()
 
     def _admit(self, job: Job, now: float) -> bool:
-        need = ctx_bytes(job)
+        need = self.bytes_of(job)
         if self.used + need > self.budget:
             return False
         b = self.batches[job.precision]
@@ -147,7 +154,7 @@ class Server:
                     job.track = b.track(slot)
                     job.done = now
                     b.remove(slot)
-                    self.used -= ctx_bytes(job)
+                    self.used -= self.bytes_of(job)
                     del self.active[prec][slot]
                     done.append(job)
 
