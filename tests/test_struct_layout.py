@@ -51,3 +51,12 @@ def test_ctypes_mirror_matches_header(name):
 @pytest.mark.parametrize("name", ["pf_grid", "pf_params"])
 def test_fortran_binding_matches_header(name):
     assert fortran_type(name) == header_struct(name)
+
+
+def test_fortran_interfaces_name_declared_entry_points():
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    hdr = open(os.path.join(ROOT, "include", "pf3d.h")).read()
+    names = set(re.findall(r'bind\(C, name="(\w+)"\)', doc))
+    assert len(names) >= 10
+    for n in names:
+        assert re.search(r"\b%s\(" % n, hdr), n
