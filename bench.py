@@ -10,11 +10,11 @@ ours       value = GCell-updates/s of the fused FP64 step, device-resident
            (CUDA events, max over ranks); e2e = the same job through the C-ABI
            with the state uploaded from / downloaded to pinned host memory and
            a per-step probe read; roofline of the dominant kernel from CUDA
-           events around each launch; cpu_baseline = the CPU oracle on a
-           bounded sample (rank 0, N = 1).
+           events around each launch; cpu_baseline = the CPU oracle on the
+           same full grid for a bounded number of steps (rank 0, N = 1).
 reference  the reference's CPU path, i.e. the CPU oracle (C restatement of
-           the Fortran OpenMP path; the Fortran cannot be compiled here) on all
-           host threads, rank 0 only.
+           the Fortran OpenMP path; the Fortran cannot be compiled here) on the
+           same full grid, all host threads, rank 0 only, K steps after W.
 Multi-GPU: the path shards by domain (replicas only): every rank runs its own
 domain, no data-path collective; value = all ranks' cell updates / max time.
 """
@@ -44,7 +44,6 @@ STEP_BYTES_PER_CELL = {64: 64, 32: 32}
 # The passes also move phi_mid, the noise hand-over and a second read of c
 # (104 B/cell in FP64 by design); ncu's per-launch DRAM bytes are "traffic".
 PASS_BYTES_PER_CELL = {"fused_first": {64: 40, 32: 20}, "fused_last": {64: 24, 32: 12}}
-CPU_SAMPLE = (512, 512, 32)   # bounded CPU sample: bottom slab of the workload
 
 
 def measured_peaks():
@@ -122,25 +121,30 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def cpu_oracle_rate(precision_unused: int, seconds: float, warmup: int = 1, min_steps: int = 2):
-    """GCell-updates/s of the CPU oracle on the bounded sample (all host threads)."""
+def oracle_on_workload(w, st, warmup: int, steps: int = 0, seconds: float = 0.0):
+    """Time the CPU oracle (the C restatement of the reference's CPU OpenMP
+    path, all host threads) on the workload's full grid from the state `st`.
+    Runs `steps` timed steps, or, with steps = 0, as many as fit `seconds`
+    (at least 2).  Returns (GCell-updates/s, steps, seconds, threads)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
-    from pf3d import deck, init
-    w = deck.WORKLOADS["c2_512x512x1024_fp64"]
-    nx, ny, nz = CPU_SAMPLE
     p = w.params()
-    g = deck.grid(nx, ny, nz, w.dx)
-    st = init.initial_state(nx, ny, nz, w.n_bumps, w.seed, p)
-    o = pyoracle.Oracle(g, p)
-    o.load_state(st)
-    o.step(warmup)
-    n, t0 = 0, time.perf_counter()
-    while n < min_steps or time.perf_counter() - t0 < seconds:
-        o.step(1)
-        n += 1
-    dt = time.perf_counter() - t0
-    return (nx * ny * nz * n / dt / 1e9, n, dt, pyoracle.num_threads())
+    o = pyoracle.Oracle(w.grid(), p)
+    try:
+        o.load_state(st)
+        o.step(warmup)
+        n, t0 = 0, time.perf_counter()
+        if steps > 0:
+            o.step(steps)
+            n = steps
+        else:
+            while n < 2 or time.perf_counter() - t0 < seconds:
+                o.step(1)
+                n += 1
+        dt = time.perf_counter() - t0
+    finally:
+        o.close()
+    return w.cells * n / dt / 1e9, n, dt, pyoracle.num_threads()
 
 
 def workload_config(w, p, world: int) -> dict:
@@ -151,31 +155,24 @@ def workload_config(w, p, world: int) -> dict:
 
 
 def run_reference(args, rank: int, world: int):
+    """The reference's CPU path on the same workload as our arm: the oracle on
+    the full grid, all host threads.  Imports only the package's host-side
+    modules (deck, initial-state recipe); libpf3d.so is never mapped."""
     if rank != 0:
         return 0
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle
     from pf3d import deck, init
     w = deck.WORKLOADS[args.workload]
-    nx, ny, nz = CPU_SAMPLE
     p = w.params()
-    g = deck.grid(nx, ny, nz, w.dx)
-    st = init.initial_state(nx, ny, nz, w.n_bumps, w.seed, p)
-    o = pyoracle.Oracle(g, p)
-    o.load_state(st)
-    o.step(args.warmup)
-    t0 = time.perf_counter()
-    o.step(args.steps)
-    dt = time.perf_counter() - t0
-    v = nx * ny * nz * args.steps / dt / 1e9
-    threads = pyoracle.num_threads()
-    sample = (f"{nx}x{ny}x{nz} bottom slab of the {w.nx}x{w.ny}x{w.nz} workload (same deck and seeded "
-              f"initial state), {args.steps} steps after {args.warmup} warm-up")
+    st = init.initial_state(w.nx, w.ny, w.nz, w.n_bumps, w.seed, p)
+    v, n, dt, threads = oracle_on_workload(w, st, args.warmup, steps=args.steps)
+    del st
+    sample = (f"the full {w.nx}x{w.ny}x{w.nz} workload (same deck and seeded initial state as the GPU arm), "
+              f"{n} steps after {args.warmup} warm-up, {threads} threads")
     line = {
         "metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "steps": n, "warmup": args.warmup, "ms_per_step": dt / n * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": dict(workload_config(w, p, world), sample_cells=nx * ny * nz),
+        "data": "synthetic", "config": workload_config(w, p, world),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "reference CPU OpenMP path as the C restatement in oracle/ (no Fortran compiler in the image)",
@@ -427,10 +424,9 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, n, dt, thr = cpu_oracle_rate(prec, args.cpu_seconds)
-        nx, ny, nz = CPU_SAMPLE
+        v, n, dt, thr = oracle_on_workload(w, st, 1, seconds=args.cpu_seconds)
         cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
-               "sample": f"{nx}x{ny}x{nz} bottom slab of the workload, {n} steps in {dt:.1f} s "
+               "sample": f"the full {w.nx}x{w.ny}x{w.nz} workload, {n} steps after 1 warm-up in {dt:.1f} s "
                          f"(C restatement of the reference CPU OpenMP path)"}
 
     if world > 1:

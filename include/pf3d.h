@@ -195,12 +195,14 @@ int pf_swap(pf_ctx* ctx);
    mapped fields, or a solver under a fixed device-memory budget).  The
    caller passes its own device fields (Fortran order, row pitch `pitch` >=
    nx elements, PF_FP64 doubles or PF_FP32 floats) and receives the five
-   values of pf_diagnosticos in out[5] (host).  Scratch is a static device
-   array of PF_NOALLOC_MAX_PLANES rows (about 256 KiB per device, held until
-   the process exits): nz above that limit is rejected with PF_E_ARG.  The
-   first call on each device looks up the array's device address, so make it
-   before any stream capture.  All calls share the array: calls whose work
-   overlaps on the GPU race.  `stream` is a cudaStream_t or NULL.          */
+   values of pf_diagnosticos in out[5] (host); the call waits on `stream`
+   for them before it returns.  Scratch is a static device array of
+   PF_NOALLOC_MAX_PLANES rows of partials (about 256 KiB per device, held
+   until the process exits); each plane is reduced in one or more rows, so
+   nz above that limit is rejected with PF_E_ARG.  The first call on each
+   device looks up the array's device address, so make it before any stream
+   capture.  All calls share the array: calls whose work overlaps on the GPU
+   race.  `stream` is a cudaStream_t or NULL.                               */
 #define PF_NOALLOC_MAX_PLANES 4096
 int pf_diagnosticos_noalloc(const void* phase_field, const void* conc_soluto, int nx, int ny, int nz,
                             int pitch, int precision, double dx, double dy, double dz, double E0,

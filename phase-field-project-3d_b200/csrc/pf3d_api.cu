@@ -488,7 +488,7 @@ int pf_checkpoint_save(pf_ctx* ctx, const char* path)
            "checkpoint copy");
     CK(cudaEventRecord(ctx->ckpt_ev, ctx->stream), "checkpoint event");
     // the host state of the copied fields: later steps are enqueued after them
-    const CkptHeader h = ckpt_header(g, ctx->prec, ctx->st);
+    const CkptHeader h = ckpt_header(g, ctx->prec, ctx->st, ctx->p);
     const std::string file(path);
     void* data = ctx->ckpt_host;
     cudaEvent_t ev = ctx->ckpt_ev;
@@ -516,7 +516,7 @@ int pf_checkpoint_load(pf_ctx* ctx, const char* path)
     std::FILE* f = std::fopen(path, "rb");
     if (!f) return ctx_err(ctx, PF_E_ARG, std::string("pf_checkpoint_load: cannot open ") + path);
     CkptHeader h;
-    std::string why = ckpt_read_header(f, ctx->g, ctx->prec, &h);
+    std::string why = ckpt_read_header(f, ctx->g, ctx->prec, ctx->p, &h);
     const pf_grid& g = ctx->g;
     const size_t row = (size_t)g.nx * ctx->es;
     const size_t fbytes = row * g.ny * g.nz;

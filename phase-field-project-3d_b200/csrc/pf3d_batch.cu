@@ -738,7 +738,7 @@ int pf_batch_checkpoint_save(pf_batch* b, int slot, const char* path)
                               b->stream),
             "checkpoint copy");
     BCK(cudaStreamSynchronize(b->stream), "checkpoint sync");
-    const std::string why = ckpt_write(path, ckpt_header(g, b->prec, sl->st), host.data(), fbytes);
+    const std::string why = ckpt_write(path, ckpt_header(g, b->prec, sl->st, sl->p), host.data(), fbytes);
     if (!why.empty()) return berr(b, PF_E_STATE, "pf_batch_checkpoint_save: " + why);
     return PF_OK;
 }
@@ -753,7 +753,7 @@ int pf_batch_checkpoint_load(pf_batch* b, int slot, const char* path)
     if (!f) return berr(b, PF_E_ARG, std::string("pf_batch_checkpoint_load: cannot open ") + path);
     const pf_grid& g = sl->g;
     CkptHeader h;
-    std::string why = ckpt_read_header(f, g, b->prec, &h);
+    std::string why = ckpt_read_header(f, g, b->prec, sl->p, &h);
     const size_t row = (size_t)g.nx * b->es;
     const size_t fbytes = row * g.ny * g.nz;
     std::vector<char> host;

@@ -12,7 +12,9 @@
 //     double dx, dy, dz
 //     int64  it
 //     double TP, M0, Cs_eq, Cl_eq
-//     float  time
+//     float  time, 4 bytes pad
+//     uint64 deck hash (FNV-1a 64 over the deck values the step reads;
+//            0 in files written before it was recorded: not checked)
 //     pad to 128 bytes
 //   4 fields in Fortran order without row padding, 8-byte doubles (precision
 //   64) or 4-byte floats (precision 32): phase_field_old, conc_soluto_old,
@@ -35,13 +37,37 @@ struct CkptHeader {
     int64_t it;
     double TP, M0, Cs_eq, Cl_eq;
     float time;
-    char pad[128 - 8 - 6 * 4 - 3 * 8 - 8 - 4 * 8 - 4];
+    int32_t pad0;
+    uint64_t deck_hash;
+    char pad[128 - 8 - 6 * 4 - 3 * 8 - 8 - 4 * 8 - 4 - 4 - 8];
 };
 static_assert(sizeof(CkptHeader) == 128, "checkpoint header is 128 bytes");
 
 constexpr int kCkptFields[4] = {PF_PHASE_OLD, PF_CONC_OLD, PF_TOLD, PF_DPP};
 
-inline CkptHeader ckpt_header(const pf_grid& g, int prec, const pf_state& st)
+// FNV-1a 64 over the bytes of every deck value a continued run reads (the
+// physics, the TP line and its cooling rate, the sweep count, h and noise
+// forms); M0 (carried by the checkpoint's state) and the driver-only stop
+// time and output cadence are left out.  Field by field, so struct padding
+// never enters the hash.  Never 0.
+inline uint64_t ckpt_deck_hash(const pf_params& p)
+{
+    uint64_t h = 0xcbf29ce484222325ull;
+    auto mix = [&h](const void* v, size_t n) {
+        const unsigned char* b = static_cast<const unsigned char*>(v);
+        for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 0x100000001b3ull;
+    };
+    const double d[] = {p.Tm, p.T0, p.delta_H, p.Cp_s, p.D, p.AAA, p.DELTA_EPSLON, p.D_sol, p.D_liq, p.Me,
+                        p.Vm, p.R, p.C0, p.Thin_Interface, p.TP, p.taxa_resfr};
+    const float f[] = {p.Ke, p.Sigma, p.Beta, p.ajuste};
+    const int i[] = {p.n_varreduras, p.h_quintico, p.ruido_tipo, p.bc};
+    mix(d, sizeof(d));
+    mix(f, sizeof(f));
+    mix(i, sizeof(i));
+    return h ? h : 1;
+}
+
+inline CkptHeader ckpt_header(const pf_grid& g, int prec, const pf_state& st, const pf_params& p)
 {
     CkptHeader h;
     std::memset(&h, 0, sizeof(h));
@@ -60,6 +86,7 @@ inline CkptHeader ckpt_header(const pf_grid& g, int prec, const pf_state& st)
     h.Cs_eq = st.Cs_eq;
     h.Cl_eq = st.Cl_eq;
     h.time = st.time;
+    h.deck_hash = ckpt_deck_hash(p);
     return h;
 }
 
@@ -86,15 +113,17 @@ inline std::string ckpt_write(const std::string& path, const CkptHeader& h, cons
     return ok ? std::string() : "short write to " + path;
 }
 
-// reads the header; checks magic, field count and that the grid and the
-// precision are the expected ones; "" on success
-inline std::string ckpt_read_header(std::FILE* f, const pf_grid& g, int prec, CkptHeader* h)
+// reads the header; checks magic, field count and that the grid (cells and
+// spacing), the precision and the deck are the expected ones; "" on success
+inline std::string ckpt_read_header(std::FILE* f, const pf_grid& g, int prec, const pf_params& p, CkptHeader* h)
 {
     if (std::fread(h, sizeof(*h), 1, f) != 1) return "checkpoint shorter than its header";
     if (std::memcmp(h->magic, "PF3DCKP1", 8) != 0) return "not a checkpoint file";
     if (h->nfields != 4) return "unsupported field count";
     if (h->precision != prec) return "checkpoint precision differs from the domain's";
     if (h->nx != g.nx || h->ny != g.ny || h->nz != g.nz) return "checkpoint grid differs from the domain's";
+    if (h->dx != g.dx || h->dy != g.dy || h->dz != g.dz) return "checkpoint grid spacing differs from the domain's";
+    if (h->deck_hash != 0 && h->deck_hash != ckpt_deck_hash(p)) return "checkpoint deck differs from the domain's";
     return std::string();
 }
 

@@ -11,13 +11,18 @@
 // pf_diagnosticos_noalloc takes the caller's device pointers and uses a
 // file-scope static device array as its scratch instead.
 //
-// The scratch holds one row of partials per z plane, so the domain may have
-// at most PF_NOALLOC_MAX_PLANES planes (4096; the array is 4097 x 8 doubles,
-// about 256 KiB, held by every device that loads the library until the
-// process exits).  Every call shares the array and leaves its contents behind;
-// each call writes every partial it later reads (rows 0 .. nz-1 and the
-// result row) before reading it, so nothing needs clearing, but two calls
-// whose work overlaps on the GPU race on the array.
+// The scratch holds up to PF_NOALLOC_MAX_PLANES rows of partials (4096; the
+// array is 4097 x 8 doubles, about 256 KiB, held by every device that loads
+// the library until the process exits).  Each z plane is split into S equal
+// runs of cells, S = min(4096 / nz, planes cells / 1024) but at least 1, and
+// one CTA reduces each run into its row, so a shallow domain still spreads
+// over the whole GPU (16 planes of 4096 x 4096 cells give 4096 CTAs of 64 Ki
+// cells each); the domain may therefore have at most 4096 planes.  The split
+// depends only on nx, ny and nz, so the summation order -- and the result --
+// is the same on every call.  Every call shares the array and leaves its
+// contents behind; each call writes every partial it later reads (rows
+// 0 .. nz*S-1 and the result row) before reading it, so nothing needs
+// clearing, but two calls whose work overlaps on the GPU race on the array.
 #include <cuda_runtime.h>
 #include <cfloat>
 #include <cmath>
@@ -36,7 +41,7 @@ constexpr int kMaxPlanes = PF_NOALLOC_MAX_PLANES;
 constexpr int kRow = 8;           // l2, l2 comp, max, min, sol, sol comp, fe, fe comp
 constexpr int kMaxDevices = 64;
 
-// rows 0 .. kMaxPlanes-1: partials of each plane; row kMaxPlanes: the result
+// rows 0 .. kMaxPlanes-1: partials of each run of cells; row kMaxPlanes: the result
 static __device__ __align__(256) double g_diag_scratch[(kMaxPlanes + 1) * kRow];
 
 std::mutex g_setup_mu;
@@ -60,20 +65,26 @@ struct NSum {
 
 struct PlaneArgs {
     int nx, ny, nz;
+    int runs;              // S: runs of cells per plane, one CTA and one row each
+    long long run;         // cells per run (the last run of a plane may be shorter)
     long long px, plane;
     double dx, dy, dz, E0, W0;
 };
 
-// one CTA per z plane, fixed reduction order (diag_body.inc:8-22 per cell)
+// one CTA per run of cells of one z plane (row blockIdx.x = z * S + s),
+// fixed reduction order (diag_body.inc:8-22 per cell)
 template <typename T>
 __global__ void __launch_bounds__(256) k_diag_plane(PlaneArgs a, const T* __restrict__ phi, const T* __restrict__ c,
                                                    double* __restrict__ part)
 {
-    const int z = blockIdx.x;
+    const int row = blockIdx.x;
+    const int z = row / a.runs, s = row % a.runs;
     NSum l2{0, 0}, sol{0, 0}, fe{0, 0};
     double mx = -DBL_MAX, mn = DBL_MAX;
     const long long ncell = (long long)a.nx * a.ny;
-    for (long long q = threadIdx.x; q < ncell; q += blockDim.x) {
+    const long long q0 = (long long)s * a.run;
+    const long long q1 = q0 + a.run < ncell ? q0 + a.run : ncell;
+    for (long long q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
         const int x = (int)(q % a.nx), y = (int)(q / a.nx);
         const long long id = (long long)x + (long long)y * a.px + (long long)z * a.plane;
         const double p = (double)phi[id];
@@ -114,17 +125,17 @@ __global__ void __launch_bounds__(256) k_diag_plane(PlaneArgs a, const T* __rest
             NSum s2{v[4], v[5]}; s2.merge(sh[ww][4], sh[ww][5]); v[4] = s2.s; v[5] = s2.c;
             NSum s3{v[6], v[7]}; s3.merge(sh[ww][6], sh[ww][7]); v[6] = s3.s; v[7] = s3.c;
         }
-        for (int k = 0; k < kRow; ++k) part[(long long)z * kRow + k] = v[k];
+        for (int k = 0; k < kRow; ++k) part[(long long)row * kRow + k] = v[k];
     }
 }
 
-__global__ void k_diag_plane_final(const double* __restrict__ part, int nz, double* __restrict__ res)
+__global__ void k_diag_plane_final(const double* __restrict__ part, int rows, double* __restrict__ res)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     NSum l2{0, 0}, sol{0, 0}, fe{0, 0};
     double mx = -DBL_MAX, mn = DBL_MAX;
-    for (int z = 0; z < nz; ++z) {
-        const double* p = part + (long long)z * kRow;
+    for (int r = 0; r < rows; ++r) {
+        const double* p = part + (long long)r * kRow;
         l2.merge(p[0], p[1]);
         mx = fmax(mx, p[2]);
         mn = fmin(mn, p[3]);
@@ -184,15 +195,22 @@ extern "C" int pf_diagnosticos_noalloc(const void* phase_field, const void* conc
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     PlaneArgs a;
     a.nx = nx; a.ny = ny; a.nz = nz;
+    const long long ncell = (long long)nx * ny;
+    long long runs = ncell / 1024;                       // at least 1024 cells a CTA
+    if (runs > kMaxPlanes / nz) runs = kMaxPlanes / nz;  // at most kMaxPlanes rows
+    if (runs < 1) runs = 1;
+    a.runs = (int)runs;
+    a.run = (ncell + runs - 1) / runs;
+    const int rows = nz * a.runs;
     a.px = pitch;
     a.plane = (long long)pitch * ny;
     a.dx = dx; a.dy = dy; a.dz = dz; a.E0 = E0; a.W0 = W0;
     double* res = scratch + (long long)kMaxPlanes * kRow;
     if (precision == PF_FP64)
-        k_diag_plane<double><<<nz, 256, 0, st>>>(a, (const double*)phase_field, (const double*)conc_soluto, scratch);
+        k_diag_plane<double><<<rows, 256, 0, st>>>(a, (const double*)phase_field, (const double*)conc_soluto, scratch);
     else
-        k_diag_plane<float><<<nz, 256, 0, st>>>(a, (const float*)phase_field, (const float*)conc_soluto, scratch);
-    k_diag_plane_final<<<1, 32, 0, st>>>(scratch, nz, res);
+        k_diag_plane<float><<<rows, 256, 0, st>>>(a, (const float*)phase_field, (const float*)conc_soluto, scratch);
+    k_diag_plane_final<<<1, 32, 0, st>>>(scratch, rows, res);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(out, res, 5 * sizeof(double), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);

@@ -1,7 +1,9 @@
 """ctypes mirror of include/pf3d.h and the loader of the in-tree libpf3d.so.
 
 The library is required: there is no Python or CPU fallback for any entry
-point.  If libpf3d.so is missing the import of this module raises.
+point.  It is mapped on the first call through `LIB` (importing the package
+for its host-side modules -- the deck and the initial-state recipe -- maps
+nothing); if libpf3d.so is missing that first call raises ImportError.
 """
 from __future__ import annotations
 
@@ -154,7 +156,23 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     return lib
 
 
-LIB = load_library()
+class _LazyLib:
+    """Forwards attribute access to libpf3d.so, loading it on first use."""
+
+    _lib = None
+
+    def __getattr__(self, name):
+        lib = _LazyLib._lib
+        if lib is None:
+            lib = _LazyLib._lib = load_library()
+        return getattr(lib, name)
+
+    @property
+    def loaded(self) -> bool:
+        return _LazyLib._lib is not None
+
+
+LIB = _LazyLib()
 
 
 class PFError(RuntimeError):

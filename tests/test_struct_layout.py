@@ -1,7 +1,7 @@
 """The structs of include/pf3d.h, their ctypes mirrors (pf3d._abi) and the
-Fortran interface types documented for the reference list
-the same fields, in the same order, with the same C types: a caller's struct
-must have the library's layout."""
+Fortran interface module for the reference (include/pf3d_bind.f90) list the
+same fields, in the same order, with the same C types: a caller's struct must
+have the library's layout."""
 import ctypes as C
 import os
 import re
@@ -29,8 +29,12 @@ def header_struct(name):
     return out
 
 
+def fortran_source():
+    return open(os.path.join(ROOT, "include", "pf3d_bind.f90")).read()
+
+
 def fortran_type(name):
-    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    doc = fortran_source()
     body = re.search(r"type, bind\(C\) :: %s[^\n]*\n(.*?)\n\s*end type" % name, doc, flags=re.S).group(1)
     out = []
     for line in body.splitlines():
@@ -54,7 +58,7 @@ def test_fortran_binding_matches_header(name):
 
 
 def test_fortran_interfaces_name_declared_entry_points():
-    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    doc = fortran_source()
     hdr = open(os.path.join(ROOT, "include", "pf3d.h")).read()
     names = set(re.findall(r'bind\(C, name="(\w+)"\)', doc))
     assert len(names) >= 10

@@ -100,6 +100,8 @@ def test_checkpoint_continues_bit_identical(gpu, prec, tmp_path):
 
 
 def test_checkpoint_rejects_other_grid_or_precision(gpu, tmp_path):
+    """A checkpoint loads only into a domain of the same precision, cells,
+    grid spacing and deck; anything else is an error, not a silent mix."""
     g, p, st = case(20, 16, 14)
     path = str(tmp_path / "b.ckpt")
     with pf3d.Domain(g, p, pf3d.PF_FP64) as a:
@@ -111,6 +113,13 @@ def test_checkpoint_rejects_other_grid_or_precision(gpu, tmp_path):
         d.restore(path)
     with pf3d.Domain(g, p, pf3d.PF_FP64) as d, pytest.raises(pf3d.PFError):
         d.restore(str(tmp_path / "missing.ckpt"))
+    with pf3d.Domain(deck.grid(20, 16, 14, 0.25e-6), p, pf3d.PF_FP64) as d, pytest.raises(pf3d.PFError):
+        d.restore(path)
+    p2 = deck.params_copy(p, taxa_resfr=p.taxa_resfr * 2)
+    with pf3d.Domain(g, p2, pf3d.PF_FP64) as d, pytest.raises(pf3d.PFError):
+        d.restore(path)
+    with pf3d.Domain(g, deck.params_copy(p, stoptime=1.0), pf3d.PF_FP64) as d:
+        d.restore(path)   # driver-only values do not enter the deck check
 
 
 @pytest.mark.parametrize("prec", PRECS)

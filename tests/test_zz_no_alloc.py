@@ -68,6 +68,48 @@ def test_noalloc_matches_pf_diagnosticos_twice(gpu, precision):
             assert abs(a - b) <= RTOL * abs(b), (got, want)
 
 
+def _exact(phi, c, dx, dy, dz, E0, W0):
+    """diag_body.inc:8-22 with exactly rounded sums (math.fsum): L2, max,
+    min, total solute, free energy (gradient term on interior cells only)."""
+    import math
+    nz, ny, nx = phi.shape
+    g2 = np.zeros_like(phi)
+    if nx > 2 and ny > 2 and nz > 2:
+        gx = (phi[1:-1, 1:-1, 2:] - phi[1:-1, 1:-1, :-2]) * 0.5 / dx
+        gy = (phi[1:-1, 2:, 1:-1] - phi[1:-1, :-2, 1:-1]) * 0.5 / dy
+        gz = (phi[2:, 1:-1, 1:-1] - phi[:-2, 1:-1, 1:-1]) * 0.5 / dz
+        g2[1:-1, 1:-1, 1:-1] = gx * gx + gy * gy + gz * gz
+    w = W0 * phi * phi * (1.0 - phi) * (1.0 - phi)
+    e = (0.5 * E0 * E0 * g2 + w) * dx * dy * dz
+    return (math.sqrt(math.fsum((phi * phi).ravel())), float(phi.max()), float(phi.min()),
+            math.fsum(c.ravel()), math.fsum(e.ravel()))
+
+
+@pytest.mark.parametrize("shape", [(5, 4, 1), (5, 4, 2), (4, 4, _abi.PF_NOALLOC_MAX_PLANES)])
+def test_noalloc_edge_shapes(gpu, shape):
+    # one plane and two planes (no interior cell: the gradient term is zero
+    # everywhere) and a thin domain whose rows fill the whole scratch, the
+    # result row right after the last partial row; each called twice
+    import torch
+    nx, ny, nz = shape
+    rng = np.random.default_rng(nx * 100 + nz)
+    phi = rng.uniform(0.0, 1.0, (nz, ny, nx))
+    c = 0.0196 * (1.0 - 0.86 * phi) + rng.normal(0.0, 1e-4, phi.shape)
+    dx = dy = dz = 0.5e-6
+    E0, W0 = 2.5e-4, 3.1e6
+    want = _exact(phi, c, dx, dy, dz, E0, W0)
+    tphi = torch.from_numpy(phi).cuda()
+    tc = torch.from_numpy(c).cuda()
+    torch.cuda.synchronize()
+    for _ in range(2):
+        out = (C.c_double * 5)()
+        _abi.check(_abi.LIB.pf_diagnosticos_noalloc(C.c_void_p(tphi.data_ptr()), C.c_void_p(tc.data_ptr()), nx, ny,
+                                                    nz, nx, pf3d.PF_FP64, dx, dy, dz, E0, W0, None, out))
+        got = tuple(out)
+        for a, b in zip(got, want):
+            assert abs(a - b) <= RTOL * abs(b), (got, want)
+
+
 def test_noalloc_rejects_more_planes_than_its_scratch(gpu):
     out = (C.c_double * 5)()
     nz = _abi.PF_NOALLOC_MAX_PLANES + 1
