@@ -264,17 +264,30 @@ def bench_karma(args, torch, stream):
 
 
 def bench_serve(args, serve):
-    """Bounded sample of the serving configuration (5): the first requests of
-    the seeded Poisson stream, every step count scaled by step_scale."""
+    """The serving configuration (5): the seeded Poisson stream of 2000
+    requests at 20/s under the 150 GB budget, every step count scaled by
+    step_scale (1 = as configured)."""
     jobs = serve.request_stream(seed=4, n=args.serve_requests, step_scale=args.serve_step_scale)
-    srv = serve.Server(budget_bytes=150e9, quantum=8)
+    srv = serve.Server(budget_bytes=150e9, quantum=args.serve_quantum)
     try:
         st = srv.run(jobs)
     finally:
         srv.close()
-    st.update({"workload": "c5_poisson_20_per_s_seed4", "sample": f"first {len(jobs)} requests, steps x {args.serve_step_scale}",
-               "fp64_share": sum(1 for j in jobs if j.precision == 64) / len(jobs), "budget_gb": 150})
+    scale = "as configured" if args.serve_step_scale == 1.0 else f"every step count x {args.serve_step_scale}"
+    st.update({"workload": "c5_poisson_20_per_s_seed4",
+               "sample": f"{len(jobs)} requests of the seeded stream, {scale}",
+               "fp64_share": sum(1 for j in jobs if j.precision == 64) / len(jobs), "quantum_steps": args.serve_quantum})
     return st
+
+
+def bench_fp32_error(args):
+    """FP32 against FP64 on the 256x256x512 replica (seed 2): worst relative
+    errors of tip position, solid fraction, tip velocity and L2(phi, c)."""
+    from pf3d import study
+    r = study.run(256, 256, 512, steps=args.error_steps, every=max(1, args.error_steps // 4), seed=2, n_bumps=16)
+    return {"workload": "c3_replica_256x256x512_seed2", "steps": r["steps"], "windows": len(r["windows"]),
+            "worst_rel_error": r["worst"], "bound_tip_and_solid_fraction": 5e-3,
+            "tip_cells": [r["windows"][0]["tip_64"], r["windows"][-1]["tip_64"]], "wall_s": r["wall_s"]}
 
 
 def main():
@@ -291,8 +304,11 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-karma", action="store_true")
-    ap.add_argument("--serve-requests", type=int, default=200)
-    ap.add_argument("--serve-step-scale", type=float, default=0.05)
+    ap.add_argument("--no-error", action="store_true")
+    ap.add_argument("--error-steps", type=int, default=2000)
+    ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-step-scale", type=float, default=0.25)
+    ap.add_argument("--serve-quantum", type=int, default=16)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -417,6 +433,8 @@ def main():
         from pf3d import serve as serve_mod
         if not args.no_batch:
             extra["batched"] = bench_batch(args, pf3d, serve_mod, init)
+        if not args.no_error:
+            extra["fp32_error"] = bench_fp32_error(args)
         if not args.no_serve:
             extra["serving"] = bench_serve(args, serve_mod)
         if not args.no_karma:

@@ -37,6 +37,13 @@ extern "C" {
 #define PF_E_NOMEM (-3)    /* device allocation refused or over budget      */
 #define PF_E_STATE (-4)    /* call not valid in the current state           */
 #define PF_E_NODEV (-5)    /* no CUDA device visible                        */
+#define PF_E_NONFINITE (-7) /* the diagnostics found cells whose phi or c is
+                              not finite (the run has blown up); the five
+                              values are still returned, max/min as NaN   */
+#define PF_E_KERNEL (-6)   /* a kernel reported a failure in the context's
+                              status word (a TMA plane load that did not
+                              arrive within its bounded wait); reported by
+                              the next pf_sync / pf_download / diagnostics  */
 
 /* field ids: the seven resident arrays of source/principal.f90:61-63 */
 #define PF_PHASE_OLD 0     /* phase_field_old */
@@ -142,6 +149,14 @@ int pf_set_stream(pf_ctx* ctx, void* stream);
 #define PF_OPT_PAIRED 5    /* two cells per thread on 32 x 8 fused tiles
                               (same results): 1 (default) in FP32, where it
                               is faster; 2 in both precisions; 0 never      */
+#define PF_OPT_KERNEL 6    /* fused passes on 32 x 8 tiles: 1 (default) TMA
+                              plane loads on mbarriers, uniform per-cell
+                              arithmetic with fan-out boundary stores; 0 the
+                              element-wise cp.async passes.  Same results.  */
+#define PF_OPT_NSLOT 7     /* node-window planes of the TMA passes: 3 (two
+                              barriers a plane, less shared memory) or 4
+                              (one barrier); 0 (default) = 3 in FP64, 4 in
+                              FP32                                          */
 int pf_set_option(pf_ctx* ctx, int opt, int value);
 int pf_get_option(const pf_ctx* ctx, int opt, int* value);
 /* With PF_OPT_KTIMING on: launches and summed device milliseconds of the
@@ -180,7 +195,9 @@ int pf_concentracao_soluto(pf_ctx* ctx);
 /* auxiliar.f90 with the context's E0/W0/parameters.                       */
 int pf_auxiliar(const pf_ctx* ctx, double TP, double Cs_eq, double Cl_eq, double* M0);
 /* diagnosticos.f90: out = {L2_phi, phi_max, phi_min, solute_total,
-   free_energy} of phase_field_new / conc_soluto_new.                      */
+   free_energy} of phase_field_new / conc_soluto_new.  Watchdog: the same
+   reduction counts the cells whose phi or c is not finite; if any, max/min
+   come back NaN and the call returns PF_E_NONFINITE (out still filled).    */
 int pf_diagnosticos(pf_ctx* ctx, double out[5]);
 /* principal.f90:200-226: old <- new for phi, T and c.  Done by exchanging
    buffers: afterwards the "new" arrays hold the previous "old" data until
@@ -260,7 +277,8 @@ int pf_shift_frame(pf_ctx* ctx, int k_desl);
    kernels, starting from the context's pf_state.  Results equal the
    sequence of per-subroutine calls above.                                 */
 int pf_step(pf_ctx* ctx, int n_steps);
-/* Same, and also fills out[5] with the diagnostics of the final state.    */
+/* Same, and also fills out[5] with the diagnostics of the final state
+   (PF_E_NONFINITE, out filled, if that state holds a non-finite value).   */
 int pf_step_diag(pf_ctx* ctx, int n_steps, double out[5]);
 
 /* ---- batches of independent domains ---------------------------------- */
@@ -286,6 +304,9 @@ int pf_batch_init_seeded(pf_batch* b, int slot, int n_bumps, const double* sites
 /* the slot stops advancing once it has completed target_it steps (0: never) */
 int pf_batch_set_target(pf_batch* b, int slot, long long target_it);
 int pf_batch_get_state(const pf_batch* b, int slot, pf_state* out);
+/* the step count (pf_state.it) of slots 0 .. n-1 in one call, -1 for a
+   free slot: what a serving loop polls every quantum                      */
+int pf_batch_progress(const pf_batch* b, int* it, int n);
 /* advance every active slot by up to n_steps steps                        */
 int pf_batch_step(pf_batch* b, int n_steps);
 /* the same without waiting: the steps are queued on the batch's stream (the
@@ -296,15 +317,23 @@ int pf_batch_wait(pf_batch* b);
 /* device milliseconds of the last pf_batch_step call (all its graphs)      */
 double pf_batch_last_ms(const pf_batch* b);
 int pf_batch_set_tile(pf_batch* b, int tile_y, int zchunk);
-/* FP32 batches on 32 x 8 tiles: 1 runs two cells per thread (same results),
-   0 one; batches with the smooth noise or heat diffusion always run one    */
+/* 32 x 8 tiles: 1 runs two cells per thread (same results), 0 one.  The
+   TMA passes pair cells in either precision, except in batches with the
+   smooth noise; the cp.async passes pair FP32 batches without the smooth
+   noise or heat diffusion only                                             */
 int pf_batch_set_paired(pf_batch* b, int paired);
-/* Autotuner: times every tile height (4, 8, 16) x z-chunk (16, 32, 64, 128)
-   -- and in FP32, for 32 x 8 tiles, one or two cells per thread -- on real
-   steps (the results do not depend on these choices; each candidate
-   advances the batch by 1 + steps_per_candidate steps), keeps the fastest
-   and caches it per shape class (precision, median column size and depth) */
+/* Which fused passes a batch runs (same results): kernel 1 (default) the
+   TMA-staged passes on 32 x 8 tiles, 0 the element-wise cp.async passes;
+   nslot as PF_OPT_NSLOT (0 = per precision)                               */
+int pf_batch_set_kernel(pf_batch* b, int kernel, int nslot);
+/* Autotuner: times every tile shape x z-chunk (16, 32, 64, 128) x one or
+   two cells per thread -- tile heights 4, 8 and 16 for the cp.async passes,
+   32 x 8 for the TMA passes -- on real steps (the results do not depend on
+   these choices; each candidate advances the batch by 1 +
+   steps_per_candidate steps), keeps the fastest and caches it per shape
+   class (precision, median column size and depth)                         */
 int pf_batch_autotune(pf_batch* b, int steps_per_candidate, int* tile_y, int* zchunk, double* ms_per_step);
+/* pf_diagnosticos of one slot's state (the watchdog as there)             */
 int pf_batch_diagnosticos(pf_batch* b, int slot, double out[5]);
 /* pf_track of one slot                                                    */
 int pf_batch_track(pf_batch* b, int slot, double out[3]);

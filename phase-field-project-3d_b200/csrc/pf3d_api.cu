@@ -19,6 +19,8 @@
 #include "pf3d_hostdesc.h"
 #include "pf3d_init.cuh"
 #include "pf3d_ckpt.h"
+#include "pf3d_tma.cuh"
+#include "pf3d_tmap.h"
 
 using namespace pf3d;
 
@@ -69,6 +71,12 @@ struct pf_ctx {
     cudaStream_t own_stream;
     cudaStream_t stream;
     int fused, tile_y, zchunk, ktiming, paired;
+    int kernel;              // PF_OPT_KERNEL: 1 TMA-staged march passes, 0 the cp.async passes
+    int nslot;               // PF_OPT_NSLOT: node-window planes of the march passes (0: per precision)
+    CUtensorMap tmap[2];     // tensor maps of the two phase-field buffers (32 x 8 march tiles)
+    void* tmap_buf[2];       // their base addresses
+    int tmap_ok;
+    int* d_status;           // kernel status word: 0, or the code a kernel left there
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_first, ev_last;
     std::string err;
     int device;
@@ -149,8 +157,8 @@ int pf_create(const pf_grid* g, const pf_params* p, int precision, pf_ctx** out)
     ctx->field_bytes = round_up((size_t)px * g->ny * g->nz * ctx->es + 64, 256);
     ctx->nblk = 592;
     const size_t track_words = round_up((size_t)g->nz + 1, 4) + 4;
-    size_t total = 7 * ctx->field_bytes + (size_t)ctx->nblk * 8 * sizeof(double) + 8 * sizeof(double) +
-                   track_words * sizeof(unsigned long long);
+    size_t total = 7 * ctx->field_bytes + (size_t)ctx->nblk * kDiagRow * sizeof(double) + 8 * sizeof(double) +
+                   track_words * sizeof(unsigned long long) + 16;
     cudaError_t e = cudaMalloc(&ctx->base, total);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -159,9 +167,10 @@ int pf_create(const pf_grid* g, const pf_params* p, int precision, pf_ctx** out)
     }
     for (int f = 0; f < 7; ++f) ctx->fld[f] = (char*)ctx->base + (size_t)f * ctx->field_bytes;
     ctx->d_part = (double*)((char*)ctx->base + 7 * ctx->field_bytes);
-    ctx->d_out = ctx->d_part + (size_t)ctx->nblk * 8;
+    ctx->d_out = ctx->d_part + (size_t)ctx->nblk * kDiagRow;
     ctx->d_track = (unsigned long long*)(ctx->d_out + 8);
     ctx->d_track_out = (double*)(ctx->d_track + round_up((size_t)g->nz + 1, 4));
+    ctx->d_status = (int*)(ctx->d_track_out + 4);
     if ((e = cudaMemset(ctx->base, 0, total)) != cudaSuccess ||
         (e = cudaMallocHost(&ctx->h_out, 8 * sizeof(double))) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess) {
@@ -170,6 +179,17 @@ int pf_create(const pf_grid* g, const pf_params* p, int precision, pf_ctx** out)
         return set_global_err(PF_E_CUDA, std::string("context set-up: ") + cudaGetErrorString(e));
     }
     ctx->stream = ctx->own_stream;
+    // tensor maps of the phase-field buffers for the TMA plane loads; without
+    // them (driver entry point missing) the step uses the cp.async passes
+    ctx->kernel = 1;
+    ctx->nslot = 0;
+    ctx->tmap_ok = 1;
+    for (int b = 0; b < 2; ++b) {
+        ctx->tmap_buf[b] = ctx->fld[b == 0 ? PF_PHASE_OLD : PF_PHASE_NEW];
+        if (encode_field_map(&ctx->tmap[b], ctx->tmap_buf[b], (int)ctx->es, g->nx, g->ny, g->nz, px,
+                             march_box_x((int)ctx->es), march_box_y(8)) != 0)
+            ctx->tmap_ok = 0;
+    }
     *out = ctx;
     return PF_OK;
 }
@@ -219,11 +239,24 @@ int pf_set_state(pf_ctx* ctx, const pf_state* st)
     return PF_OK;
 }
 
+// the kernel status word, after the stream has drained: PF_E_KERNEL when a
+// kernel reported a failure (the word is cleared after it is reported)
+static int kernel_status(pf_ctx* ctx)
+{
+    int code = 0;
+    CK(cudaMemcpyAsync(&code, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "status read");
+    CK(cudaStreamSynchronize(ctx->stream), "status read");
+    if (code == 0) return PF_OK;
+    CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream), "status reset");
+    return ctx_err(ctx, PF_E_KERNEL, "a kernel reported failure code " + std::to_string(code) +
+                                         (code == kErrTmaTimeout ? " (a TMA plane load did not arrive in time)" : ""));
+}
+
 int pf_sync(pf_ctx* ctx)
 {
     if (!ctx) return PF_E_ARG;
     CK(cudaStreamSynchronize(ctx->stream), "pf_sync");
-    return PF_OK;
+    return kernel_status(ctx);
 }
 
 int pf_set_stream(pf_ctx* ctx, void* stream)
@@ -251,6 +284,14 @@ int pf_set_option(pf_ctx* ctx, int opt, int value)
         if (value < 0 || value > 2) return ctx_err(ctx, PF_E_ARG, "paired must be 0, 1 or 2");
         ctx->paired = value;
         return PF_OK;
+    case PF_OPT_KERNEL:
+        if (value < 0 || value > 1) return ctx_err(ctx, PF_E_ARG, "kernel must be 0 or 1");
+        ctx->kernel = value;
+        return PF_OK;
+    case PF_OPT_NSLOT:
+        if (value != 0 && value != 3 && value != 4) return ctx_err(ctx, PF_E_ARG, "nslot must be 0, 3 or 4");
+        ctx->nslot = value;
+        return PF_OK;
     }
     return ctx_err(ctx, PF_E_ARG, "unknown option");
 }
@@ -264,6 +305,8 @@ int pf_get_option(const pf_ctx* ctx, int opt, int* value)
     case PF_OPT_ZCHUNK: *value = ctx->zchunk; return PF_OK;
     case PF_OPT_KTIMING: *value = ctx->ktiming; return PF_OK;
     case PF_OPT_PAIRED: *value = ctx->paired; return PF_OK;
+    case PF_OPT_KERNEL: *value = ctx->kernel; return PF_OK;
+    case PF_OPT_NSLOT: *value = ctx->nslot; return PF_OK;
     }
     return PF_E_ARG;
 }
@@ -328,7 +371,7 @@ int pf_download(pf_ctx* ctx, int field, double* host)
         }
     }
     CK(cudaStreamSynchronize(ctx->stream), "pf_download sync");
-    return PF_OK;
+    return kernel_status(ctx);
 }
 
 int pf_probe(pf_ctx* ctx, int field, int i, int j, int k, double* value)
@@ -423,9 +466,14 @@ static int run_diag(pf_ctx* ctx, const void* phi, const void* c, double out[5])
     CK(is64(ctx) ? launch_diag<double>(ctx->dd, phi, c, ctx->d_part, ctx->nblk, ctx->d_out, ctx->stream)
                  : launch_diag<float>(ctx->dd, phi, c, ctx->d_part, ctx->nblk, ctx->d_out, ctx->stream),
        "diagnosticos");
-    CK(cudaMemcpyAsync(ctx->h_out, ctx->d_out, 5 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "diag copy");
+    CK(cudaMemcpyAsync(ctx->h_out, ctx->d_out, 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "diag copy");
     CK(cudaStreamSynchronize(ctx->stream), "diag sync");
     std::memcpy(out, ctx->h_out, 5 * sizeof(double));
+    const int rc = kernel_status(ctx);
+    if (rc != PF_OK) return rc;
+    if (ctx->h_out[5] != 0.0)
+        return ctx_err(ctx, PF_E_NONFINITE, "diagnosticos: " + std::to_string((long long)ctx->h_out[5]) +
+                                                " cells hold a non-finite phi or c (the run has blown up)");
     return PF_OK;
 }
 
@@ -594,7 +642,51 @@ static int one_step(pf_ctx* ctx)
     Fields f = fields_of(ctx);
     void* final_phi;
     void* other_phi;
-    if (ctx->fused) {
+    const bool march = ctx->fused && ctx->kernel == 1 && ctx->tmap_ok && ctx->tile_y == 8;
+    if (march) {
+        // TMA-staged passes: two cells per thread unless PF_OPT_PAIRED says
+        // otherwise (default: FP32 only) or the deck draws the smooth noise
+        const int lanes = ((ctx->paired == 2 || (ctx->paired == 1 && !is64(ctx))) && p.ruido_tipo != 2) ? 2 : 1;
+        const int nslot = ctx->nslot ? ctx->nslot : (is64(ctx) ? 3 : 4);
+        auto tm_of = [ctx](const void* buf) -> const CUtensorMap& {
+            return ctx->tmap[buf == ctx->tmap_buf[0] ? 0 : 1];
+        };
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        f.phi_mid = B;
+        if (ctx->ktiming) { e0 = new_event(); e1 = new_event(); cudaEventRecord(e0, ctx->stream); }
+        CK(is64(ctx) ? launch_march_first<double>(tm_of(A), ctx->dd, s, f, nsw == 1, lanes, nslot, ctx->zchunk,
+                                                  ctx->d_status, ctx->stream)
+                     : launch_march_first<float>(tm_of(A), ctx->dd, s, f, nsw == 1, lanes, nslot, ctx->zchunk,
+                                                 ctx->d_status, ctx->stream),
+           nsw == 1 ? "march step (single sweep)" : "march heat + sweep 1");
+        if (ctx->ktiming) { cudaEventRecord(e1, ctx->stream); ctx->ev_first.push_back({e0, e1}); }
+        if (nsw == 1) {
+            final_phi = B;
+            other_phi = A;
+        } else {
+            void* cur = B;   // phase after the sweeps so far
+            void* oth = A;   // free buffer
+            for (int sw = 2; sw <= nsw - 1; ++sw) {
+                // no DPP: it carries the step's noise from the first to the last pass
+                CK(is64(ctx) ? launch_phase<double>(ctx->dd, s, cur, f.c_old, oth, nullptr, ctx->stream)
+                             : launch_phase<float>(ctx->dd, s, cur, f.c_old, oth, nullptr, ctx->stream),
+                   "middle sweep");
+                std::swap(cur, oth);
+            }
+            Fields f2 = f;
+            f2.phi_mid = cur;
+            f2.phi_new = oth;
+            if (ctx->ktiming) { e0 = new_event(); e1 = new_event(); cudaEventRecord(e0, ctx->stream); }
+            CK(is64(ctx) ? launch_march_last<double>(tm_of(cur), ctx->dd, s, f2, lanes, nslot, ctx->zchunk,
+                                                     ctx->d_status, ctx->stream)
+                         : launch_march_last<float>(tm_of(cur), ctx->dd, s, f2, lanes, nslot, ctx->zchunk,
+                                                    ctx->d_status, ctx->stream),
+               "march last sweep + solute");
+            if (ctx->ktiming) { cudaEventRecord(e1, ctx->stream); ctx->ev_last.push_back({e0, e1}); }
+            final_phi = oth;
+            other_phi = cur;
+        }
+    } else if (ctx->fused) {
         // two cells per thread on 32 x 8 tiles; the smooth noise keeps one
         const bool pair = (ctx->paired == 2 || (ctx->paired == 1 && !is64(ctx))) && ctx->tile_y == 8 &&
                           p.ruido_tipo != 2 && !ctx->dd.do_heat_lap;

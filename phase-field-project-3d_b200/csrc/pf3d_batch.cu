@@ -28,6 +28,8 @@
 #include "pf3d_hostdesc.h"
 #include "pf3d_ckpt.h"
 #include "pf3d_init.cuh"
+#include "pf3d_tma.cuh"
+#include "pf3d_tmap.h"
 
 using namespace pf3d;
 
@@ -74,16 +76,20 @@ struct pf_batch {
     int item_cap = 0;
     int* d_nitems = nullptr;
     bool items_dirty = true;
-    double* d_part = nullptr;          // diagnostics partials (592 x 8) + result
+    double* d_part = nullptr;          // diagnostics partials (592 x kDiagRow) + result
     unsigned long long* d_track = nullptr;   // tracking scratch (grown to the tallest slot tracked)
     int track_cap = 0;                 // planes it holds
     double* h_out = nullptr;
     double* d_sites = nullptr;         // bump sites for device initialisation
     int tile_y = 8, zchunk = 64, n_sm = 0;   // persistent grids: n_sm x resident CTAs
-    int pair = 0;                      // FP32 32 x 8 tiles with two cells per thread (set by the autotuner)
+    int pair = 0;                      // 32 x 8 tiles with two cells per thread (set by the autotuner)
+    int march = 1;                     // TMA-staged march passes (32 x 8 tiles); 0: the cp.async passes
+    int nslot = 0;                     // node-window planes of the march passes (0: 3 in FP64, 4 in FP32)
+    CUtensorMap* d_tmaps = nullptr;    // 2 per slot: the tensor maps of its phase-field buffers
+    int* d_status = nullptr;           // kernel status word (0, or the code a kernel left there)
     cudaStream_t own_stream = nullptr, stream = nullptr;
     cudaGraphExec_t graph = nullptr;
-    int graph_ty = 0, graph_zc = 0, graph_nsm = 0, graph_nsw = 0;
+    int graph_ty = 0, graph_zc = 0, graph_nsm = 0, graph_nsw = 0, graph_march = -1, graph_nslot = 0;
     bool graph_smooth = false, graph_pair = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
@@ -162,15 +168,22 @@ static bool any_lap(const pf_batch* b)
     return false;
 }
 
+static bool use_march(const pf_batch* b) { return b->march && b->tile_y == 8; }
+
 static int capture_graph(pf_batch* b)
 {
     const bool smooth = any_smooth(b);
-    // two cells per thread: FP32 batches on 32 x 8 tiles whose decks allow it,
-    // when the autotuner measured it faster (boundary tiles, frequent in
-    // small domains, run the one-cell code twice per thread)
-    const bool pair = b->pair && !b64(b) && b->tile_y == 8 && !smooth && !any_lap(b);
+    const bool march = use_march(b);
+    const int nslot = b->nslot ? b->nslot : (b64(b) ? 3 : 4);
+    // two cells per thread on 32 x 8 tiles when the autotuner measured it
+    // faster: the march passes in either precision (not with the smooth
+    // noise); the cp.async passes in FP32 only, on decks without heat
+    // diffusion (their boundary tiles run the one-cell code twice)
+    const bool pair = march ? (b->pair && !smooth)
+                            : (b->pair && !b64(b) && b->tile_y == 8 && !smooth && !any_lap(b));
     if (b->graph && b->graph_ty == b->tile_y && b->graph_zc == b->zchunk && b->graph_nsm == b->n_sm &&
-        b->graph_nsw == b->nsw && b->graph_smooth == smooth && b->graph_pair == pair)
+        b->graph_nsw == b->nsw && b->graph_smooth == smooth && b->graph_pair == pair &&
+        b->graph_march == (int)march && b->graph_nslot == nslot)
         return PF_OK;
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
@@ -184,6 +197,17 @@ static int capture_graph(pf_batch* b)
         for (int k = 0; k < kGraphSteps && e == cudaSuccess; ++k) {
             const BatchStep* st = b->d_steps + (size_t)k * b->max_domains;
             const bool one = b->nsw == 1;
+            if (march) {
+                const int lanes = pair ? 2 : 1;
+                for (int pass = 0; pass <= (one ? 0 : 1) && e == cudaSuccess; ++pass)
+                    e = b64(b) ? launch_march_batch<double>(b->d_doms, b->d_tmaps, st, b->d_items, b->d_nitems, pass,
+                                                            one, smooth && pass == 0, lanes, nslot, b->zchunk,
+                                                            b->n_sm, b->d_status, cs)
+                               : launch_march_batch<float>(b->d_doms, b->d_tmaps, st, b->d_items, b->d_nitems, pass,
+                                                           one, smooth && pass == 0, lanes, nslot, b->zchunk,
+                                                           b->n_sm, b->d_status, cs);
+                continue;
+            }
             if (pair) {
                 e = launch_fused_batch_pair<float>(b->d_doms, st, b->d_items, b->d_nitems, 0, one, b->zchunk, b->n_sm,
                                                    cs);
@@ -215,6 +239,8 @@ static int capture_graph(pf_batch* b)
     b->graph_nsw = b->nsw;
     b->graph_smooth = smooth;
     b->graph_pair = pair;
+    b->graph_march = (int)march;
+    b->graph_nslot = nslot;
     return PF_OK;
 }
 
@@ -305,8 +331,10 @@ int pf_batch_create(int precision, long long budget_bytes, int max_domains, pf_b
         (e = cudaMallocHost(&b->h_steps[0], step_bytes)) != cudaSuccess ||
         (e = cudaMallocHost(&b->h_steps[1], step_bytes)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_nitems, sizeof(int))) != cudaSuccess ||
-        (e = cudaMalloc(&b->d_part, (592 * 8 + 8) * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_part, (592 * kDiagRow + 8) * sizeof(double))) != cudaSuccess ||
         (e = cudaMalloc(&b->d_sites, 2 * 4096 * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_tmaps, sizeof(CUtensorMap) * 2 * (size_t)max_domains)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_status, sizeof(int))) != cudaSuccess ||
         (e = cudaMallocHost(&b->h_out, 8 * sizeof(double))) != cudaSuccess ||
         (e = cudaEventCreate(&b->h_ev[0])) != cudaSuccess || (e = cudaEventCreate(&b->h_ev[1])) != cudaSuccess ||
         (e = cudaEventCreate(&b->ev0)) != cudaSuccess || (e = cudaEventCreate(&b->ev1)) != cudaSuccess) {
@@ -329,6 +357,8 @@ int pf_batch_create(int precision, long long budget_bytes, int max_domains, pf_b
     }
     cudaMemset(b->d_steps, 0, step_bytes);
     cudaMemset(b->d_nitems, 0, sizeof(int));
+    cudaMemset(b->d_status, 0, sizeof(int));
+    if (!tmap_encoder()) b->march = 0;   // no tensor-map encoder in this driver: the cp.async passes
     set_grid(b);
     *out = b;
     return PF_OK;
@@ -350,6 +380,8 @@ int pf_batch_destroy(pf_batch* b)
     cudaFree(b->d_part);
     if (b->d_track) cudaFree(b->d_track);
     cudaFree(b->d_sites);
+    cudaFree(b->d_tmaps);
+    cudaFree(b->d_status);
     cudaFreeHost(b->h_out);
     for (cudaEvent_t ev : {b->h_ev[0], b->h_ev[1], b->ev0, b->ev1})
         if (ev) cudaEventDestroy(ev);
@@ -425,6 +457,18 @@ int pf_batch_add(pf_batch* b, const pf_grid* g, const pf_params* p, int* slot)
     sl.bd.dpp = m + 6 * fb;
     // from pageable memory: staged at the call, so no wait is needed
     BCK(cudaMemcpyAsync(b->d_doms + s, &sl.bd, sizeof(BatchDomain), cudaMemcpyHostToDevice, b->stream), "descriptor");
+    if (b->march) {
+        CUtensorMap tm[2];
+        for (int q = 0; q < 2; ++q)
+            if (encode_field_map(&tm[q], sl.bd.phi[q], (int)b->es, g->nx, g->ny, g->nz, px, march_box_x((int)b->es),
+                                 march_box_y(8)) != 0) {
+                cudaFreeAsync(mem, b->stream);
+                sl = Slot();
+                return berr(b, PF_E_CUDA, "pf_batch_add: tensor map encoding failed");
+            }
+        BCK(cudaMemcpyAsync(b->d_tmaps + 2 * (size_t)s, tm, sizeof(tm), cudaMemcpyHostToDevice, b->stream),
+            "tensor maps");
+    }
     b->used_bytes += (long long)bytes;
     b->nsw = p->n_varreduras;
     b->items_dirty = true;
@@ -557,10 +601,43 @@ int pf_batch_get_state(const pf_batch* b, int slot, pf_state* out)
     return PF_OK;
 }
 
+int pf_batch_progress(const pf_batch* b, int* it, int n)
+{
+    if (!b || !it || n < 0) return PF_E_ARG;
+    for (int s = 0; s < n; ++s)
+        it[s] = (s < (int)b->slots.size() && b->slots[s].used) ? b->slots[s].st.it : -1;
+    return PF_OK;
+}
+
 int pf_batch_set_paired(pf_batch* b, int paired)
 {
     if (!b || paired < 0 || paired > 1) return berr(b, PF_E_ARG, "pf_batch_set_paired: 0 or 1");
     b->pair = paired;
+    return PF_OK;
+}
+
+int pf_batch_set_kernel(pf_batch* b, int kernel, int nslot)
+{
+    if (!b || kernel < 0 || kernel > 1 || (nslot != 0 && nslot != 3 && nslot != 4))
+        return berr(b, PF_E_ARG, "pf_batch_set_kernel: kernel 0 or 1, nslot 0, 3 or 4");
+    if (kernel == 1 && !tmap_encoder())
+        return berr(b, PF_E_STATE, "pf_batch_set_kernel: this driver has no tensor-map encoder");
+    if (kernel == 1 && !b->march) {
+        // slots added while the march passes were off have no tensor maps yet
+        for (int s = 0; s < (int)b->slots.size(); ++s) {
+            Slot& sl = b->slots[s];
+            if (!sl.used) continue;
+            CUtensorMap tm[2];
+            for (int q = 0; q < 2; ++q)
+                if (encode_field_map(&tm[q], sl.bd.phi[q], (int)b->es, sl.g.nx, sl.g.ny, sl.g.nz, sl.bd.d.px,
+                                     march_box_x((int)b->es), march_box_y(8)) != 0)
+                    return berr(b, PF_E_CUDA, "pf_batch_set_kernel: tensor map encoding failed");
+            BCK(cudaMemcpyAsync(b->d_tmaps + 2 * (size_t)s, tm, sizeof(tm), cudaMemcpyHostToDevice, b->stream),
+                "tensor maps");
+        }
+    }
+    b->march = kernel;
+    b->nslot = nslot;
     return PF_OK;
 }
 
@@ -616,6 +693,19 @@ int pf_batch_step_async(pf_batch* b, int n_steps)
     return PF_OK;
 }
 
+// the kernel status word, after the stream has drained: PF_E_KERNEL when a
+// kernel reported a failure (cleared once reported)
+static int batch_status(pf_batch* b)
+{
+    int code = 0;
+    BCK(cudaMemcpyAsync(&code, b->d_status, sizeof(int), cudaMemcpyDeviceToHost, b->stream), "status read");
+    BCK(cudaStreamSynchronize(b->stream), "status read");
+    if (code == 0) return PF_OK;
+    BCK(cudaMemsetAsync(b->d_status, 0, sizeof(int), b->stream), "status reset");
+    return berr(b, PF_E_KERNEL, "a batch kernel reported failure code " + std::to_string(code) +
+                                    (code == kErrTmaTimeout ? " (a TMA plane load did not arrive in time)" : ""));
+}
+
 // Waits for the steps of the last pf_batch_step_async; their device time is
 // then pf_batch_last_ms.
 int pf_batch_wait(pf_batch* b)
@@ -627,7 +717,7 @@ int pf_batch_wait(pf_batch* b)
     cudaEventElapsedTime(&ms, b->ev0, b->ev1);
     b->last_ms = ms;
     b->pending = false;
-    return PF_OK;
+    return batch_status(b);
 }
 
 int pf_batch_step(pf_batch* b, int n_steps)
@@ -670,9 +760,11 @@ int pf_batch_autotune(pf_batch* b, int steps_per_candidate, int* tile_y, int* zc
     // shape), one untimed step first
     double best = 1e300;
     int bty = b->tile_y, bzc = b->zchunk, bpair = 0;
+    const bool march = b->march != 0;
     for (int ty : {4, 8, 16})
         for (int zc : {16, 32, 64, 128})
-            for (int pr = 0; pr <= ((ty == 8 && !b64(b)) ? 1 : 0); ++pr) {
+            for (int pr = 0; pr <= ((ty == 8 && (march || !b64(b))) ? 1 : 0); ++pr) {
+                if (march && ty != 8) break;   // the march passes run 32 x 8 tiles
                 int rc = pf_batch_set_tile(b, ty, zc);
                 b->pair = pr;
                 if (!rc) rc = pf_batch_step(b, 1);
@@ -776,15 +868,20 @@ int pf_batch_diagnosticos(pf_batch* b, int slot, double out[5])
 {
     Slot* sl = get_slot(b, slot);
     if (!sl || !out) return berr(b, PF_E_ARG, "pf_batch_diagnosticos: bad argument");
-    double* res = b->d_part + 592 * 8;
+    double* res = b->d_part + 592 * kDiagRow;
     cudaError_t e = b64(b) ? launch_diag<double>(sl->bd.d, slot_field(*sl, PF_PHASE_OLD), slot_field(*sl, PF_CONC_OLD),
                                                  b->d_part, 592, res, b->stream)
                            : launch_diag<float>(sl->bd.d, slot_field(*sl, PF_PHASE_OLD), slot_field(*sl, PF_CONC_OLD),
                                                 b->d_part, 592, res, b->stream);
     BCK(e, "pf_batch_diagnosticos");
-    BCK(cudaMemcpyAsync(b->h_out, res, 5 * sizeof(double), cudaMemcpyDeviceToHost, b->stream), "diag copy");
+    BCK(cudaMemcpyAsync(b->h_out, res, 6 * sizeof(double), cudaMemcpyDeviceToHost, b->stream), "diag copy");
     BCK(cudaStreamSynchronize(b->stream), "diag sync");
     std::memcpy(out, b->h_out, 5 * sizeof(double));
+    const int rc = batch_status(b);
+    if (rc != PF_OK) return rc;
+    if (b->h_out[5] != 0.0)
+        return berr(b, PF_E_NONFINITE, "pf_batch_diagnosticos: " + std::to_string((long long)b->h_out[5]) +
+                                           " cells of the slot hold a non-finite phi or c (the run has blown up)");
     return PF_OK;
 }
 

@@ -374,12 +374,19 @@ struct Nbr {
 };
 
 // phase_body.inc:133-198 given the stencil values and the six node
-// quantities.  Returns PPNEW (unclamped).
-template <typename T, bool FAST>
+// quantities.  Returns PPNEW (unclamped).  SQ (fast form only): the nodes'
+// eps member already holds eps*eps, squared once per node instead of once
+// per use (the same product, so the same bits).
+template <typename T, bool FAST, bool SQ = false>
 __device__ __forceinline__ T phase_ppnew(const Nbr<T>& p, const Node<T>& E, const Node<T>& W, const Node<T>& N,
                                           const Node<T>& S, const Node<T>& Tt, const Node<T>& B, T CPP,
                                           T ran, const KC<T>& c)
 {
+    static_assert(FAST || !SQ, "squared node values are a fast-form input");
+    auto e2 = [](const Node<T>& n) -> T {
+        if constexpr (SQ) return n.eps;
+        else return n.eps * n.eps;
+    };
     const T PP = p.PP;
     const T one = (T)1, two = (T)2;
     if constexpr (!FAST) {
@@ -420,9 +427,9 @@ __device__ __forceinline__ T phase_ppnew(const Nbr<T>& p, const Node<T>& E, cons
             ruidos = (two * (T)ran - one) * c.AAA * (T)16 * pp2 * (q * q);
         return PP + c.M0dt * (AA + GG) + ruidos;
     } else {
-        T ax = fmadd(E.eps * E.eps, p.PE - PP, W.eps * W.eps * (p.PW - PP));
-        T ay = fmadd(N.eps * N.eps, p.PN - PP, S.eps * S.eps * (p.PS - PP));
-        T az = fmadd(Tt.eps * Tt.eps, p.PT - PP, B.eps * B.eps * (p.PB - PP));
+        T ax = fmadd(e2(E), p.PE - PP, e2(W) * (p.PW - PP));
+        T ay = fmadd(e2(N), p.PN - PP, e2(S) * (p.PS - PP));
+        T az = fmadd(e2(Tt), p.PT - PP, e2(B) * (p.PB - PP));
         T AA = fmadd(ax, c.rdx2, fmadd(ay, c.rdy2, az * c.rdz2));
         // cross terms of phase_body.inc:137-147 grouped by node
         T Cxy = fmadd(E.exy, (p.PNE - p.PSE) + (p.PN - p.PS),

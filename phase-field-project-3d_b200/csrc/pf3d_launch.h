@@ -2,6 +2,7 @@
 // templates in pf3d_kernels.cuh, instantiated for double in pf3d_fp64.cu
 // (built with --fmad=false) and for float in pf3d_fp32.cu.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include "pf3d_device.cuh"
 
@@ -74,6 +75,24 @@ template <typename T> cudaError_t launch_fused_batch_pair(const BatchDomain* dom
                                                           const BatchItem* items, const int* n_items, int pass,
                                                           bool one_sweep, int zchunk, int n_sm, cudaStream_t st);
 
+// TMA-staged z-marching passes (pf3d_march.cuh): 32 x 8 tiles, the input
+// phase field through the tensor map `tm`, `lanes` cells per thread (1 or 2),
+// `nslot` node-window planes (3 or 4); a plane load that does not arrive sets
+// *err.  Same outputs, bit for bit, as launch_fused_first / _last.
+template <typename S> cudaError_t launch_march_first(const CUtensorMap& tm, const DomainDesc& d, const StepArgs& s,
+                                                     const Fields& f, bool with_solute, int lanes, int nslot,
+                                                     int zchunk, int* err, cudaStream_t st);
+template <typename S> cudaError_t launch_march_last(const CUtensorMap& tm, const DomainDesc& d, const StepArgs& s,
+                                                    const Fields& f, int lanes, int nslot, int zchunk, int* err,
+                                                    cudaStream_t st);
+// batch form: tmaps[2 d + b] is the tensor map of buffer b of domain d's
+// phase field
+template <typename S> cudaError_t launch_march_batch(const BatchDomain* doms, const CUtensorMap* tmaps,
+                                                     const BatchStep* steps, const BatchItem* items,
+                                                     const int* n_items, int pass, bool one_sweep, bool smooth,
+                                                     int lanes, int nslot, int zchunk, int n_sm, int* err,
+                                                     cudaStream_t st);
+
 // Solidification tracking of phi: out[3] = {solid fraction, tip position
 // (cells, 1-based), solid cells}; scratch holds nz + 1 words.
 template <typename T> cudaError_t launch_track(const DomainDesc& d, const void* phi, unsigned long long* scratch,
@@ -85,7 +104,10 @@ template <typename T> cudaError_t launch_shift_frame(const DomainDesc& d, int kd
                                                      void* phi_n, void* c_n, cudaStream_t st);
 template <typename T> cudaError_t launch_fill(void* a, long long n, double v, cudaStream_t st);
 
-// Diagnostics: block partials into part[nblk*8], final into out[5].
+// Diagnostics: block partials into part[nblk*kDiagRow], final into out[6]:
+// the five values of diagnosticos and the count of cells whose phi or c is
+// not finite (the watchdog).
+constexpr int kDiagRow = 10;   // l2, l2 comp, max, min, sol, sol comp, fe, fe comp, non-finite cells, pad
 template <typename T> cudaError_t launch_diag(const DomainDesc& d, const void* phi, const void* c, double* part,
                                               int nblk, double* out, cudaStream_t st);
 

@@ -1,0 +1,754 @@
+// pf3d_march.cuh -- the z-marching passes of the coupled step, TMA-staged.
+//
+// A CTA owns a 32 x TY column tile and a z-chunk and marches along z, like
+// the passes of pf3d_fused.cuh, with the same per-cell arithmetic (the fast
+// form of pf3d_device.cuh), so every output has the bits of those passes.
+// What differs is how data moves and how the boundary is treated:
+//
+//  * Plane staging.  Each plane of the input phase field (tile + 2-cell halo)
+//    is one TMA tiled load (cp.async.bulk.tensor.3d, no multicast) issued by
+//    one thread into a 6-slot window and completed on that slot's mbarrier;
+//    the loads run two planes ahead of the stencil.  Cells outside the domain
+//    read as zero.  Every wait is bounded: a load that does not arrive sets
+//    the context's status word and the CTA stops (pf3d_tma.cuh).
+//  * Node windows.  The anisotropy quantities (eps^2, exy, eyz, ezx) of every
+//    node of the tile and its 1-cell ring, and the solute point quantities
+//    (Gamma bracket, mu), are computed once per plane into NSLOT-plane
+//    windows.  With NSLOT = 4 one barrier per plane orders everything; with
+//    NSLOT = 3 (less shared memory) a second barrier closes each plane.
+//  * Uniform arithmetic, fan-out stores.  Every cell of every tile -- also
+//    the tiles on the domain boundary -- goes through the same arithmetic
+//    (two cells per thread as lane pairs when L = 2, packed f32x2 in FP32).
+//    The boundary decoration of the reference (plane copies after the sweep,
+//    equacao_campo_fase.f90:151-167, concentracao_soluto.f90:116-124) is a
+//    per-cell store fan-out: a cell writes its value to every cell whose
+//    copy source it is (one store in the interior, up to 27 at a corner).
+//    Only the stores diverge; small domains, whose tiles are all boundary
+//    tiles, run the paired arithmetic at the interior's cost.
+//
+// Template switches: HEAT (temperatura), DPPW (write DPP: last sweep), SOL
+// (concentracao_soluto from the same input phase field), SMOOTH (the deck
+// may draw the smooth noise).  The first pass of a multi-sweep step stores
+// the step's REAL(4) noise in the DPP buffer and the last pass reads it back
+// (both sweeps use the same it, so the same noise: principal.f90:127-151).
+#pragma once
+#include "pf3d_launch.h"
+#include "pf3d_pair.cuh"
+#include "pf3d_tma.cuh"
+
+namespace pf3d {
+
+// L lanes (cells) per thread: the arithmetic type and its packing
+template <typename S, int L> struct Lanes;
+template <typename S> struct Lanes<S, 1> {
+    using V = S;
+    static __device__ __forceinline__ V make(const S* a) { return a[0]; }
+    static __device__ __forceinline__ S get(const V& v, int) { return v; }
+};
+template <typename S> struct Lanes<S, 2> {
+    using V = typename PairOf<S>::type;
+    static __device__ __forceinline__ V make(const S* a) { return V(a[0], a[1]); }
+    static __device__ __forceinline__ S get(const V& v, int l) { return l ? v.y() : v.x(); }
+};
+
+// Shared-memory layout of one tile (bytes from a 128-byte aligned base).
+template <typename S, int TY, bool SOL, int NSLOT>
+struct MarchLayout {
+    static constexpr int TX = 32;
+    // the TMA box starts XOFF cells left of the tile: x * sizeof(S) must be a
+    // multiple of 16 bytes (tile origins are multiples of 32 cells)
+    static constexpr int XOFF = (sizeof(S) == 8) ? 2 : 4;
+    static constexpr int TW = TX + 2 * XOFF;       // phase tile width (box x)
+    static constexpr int PH = TY + 4;              // phase tile height (box y)
+    static constexpr int NW = TX + 2, NH = TY + 2; // node / point tile (ring 1)
+    static constexpr int NQ = NW * NH;
+    static constexpr int NPHI = 6;                 // phase planes z-1 .. z+4
+    static constexpr int PHI_SLOT = TW * PH;       // elements per phase slot
+    static constexpr int PHI_BYTES = PHI_SLOT * (int)sizeof(S);
+    static_assert(PHI_BYTES % 128 == 0, "TMA destinations are 128-byte aligned");
+    static constexpr int BAR_OFF = NPHI * PHI_BYTES;
+    static constexpr int NODE_OFF = (BAR_OFF + NPHI * 8 + 127) / 128 * 128;
+    static constexpr int NODE_SLOT = 4 * NQ;       // eps^2, exy, eyz, ezx
+    static constexpr int SOL_OFF = NODE_OFF + NSLOT * NODE_SLOT * (int)sizeof(S);
+    static constexpr int SOL_SLOT = 2 * NQ;        // Gamma bracket, mu
+    static constexpr int BYTES = SOL_OFF + (SOL ? NSLOT * SOL_SLOT * (int)sizeof(S) : 0);
+    static constexpr int ALLOC = BYTES + 128;      // slack to align the dynamic base
+};
+
+// temperatura at one own cell (temp_body.inc:31-41): the neighbours of TOLD
+// are read only when the deck has heat diffusion (D != 0)
+template <typename S>
+__device__ __forceinline__ S heat_at(const S* __restrict__ T_old, long long id, long long px, long long pl, S PP,
+                                     S dppv, const KC<S>& c)
+{
+    S TE = 0, TW = 0, TN = 0, TS = 0, TT = 0, TB = 0;
+    if (c.lap) {
+        TE = T_old[id + 1]; TW = T_old[id - 1]; TN = T_old[id + px]; TS = T_old[id - px];
+        TT = T_old[id + pl]; TB = T_old[id - pl];
+    }
+    return heat_new<S>(PP, dppv, TE, TW, TN, TS, TT, TB, c);
+}
+
+__device__ __forceinline__ unsigned char* align128(unsigned char* p)
+{
+    return reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(p) + 127) & ~uintptr_t(127));
+}
+
+// Initialises the six plane barriers of a tile's window (one thread), made
+// visible to the TMA unit and to every thread of the CTA.
+template <typename S, int TY, bool SOL, int NSLOT>
+__device__ __forceinline__ void march_init_barriers(unsigned char* smem)
+{
+    using LY = MarchLayout<S, TY, SOL, NSLOT>;
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        const uint32_t b0 = smem_u32(smem + LY::BAR_OFF);
+        for (int s = 0; s < LY::NPHI; ++s) mbar_init(b0 + 8 * s, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+}
+
+// One 32 x TY x zchunk tile (tile coordinates bx, by, bz) of one domain, read
+// from the phase field the tensor map `tm` describes.  `par` carries the
+// parity of each plane barrier across the tiles a CTA processes (every load
+// issued is waited for).  Returns false if a plane load did not arrive in
+// time; the CTA must then stop.
+template <typename S, int L, int TY, int NSLOT, bool HEAT, bool DPPW, bool SOL, bool SMOOTH>
+__device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, const KC<typename Lanes<S, L>::V>& cv,
+                                           const CUtensorMap* tm, const S* __restrict__ c_in,
+                                           S* __restrict__ phi_out, S* __restrict__ dpp, S* __restrict__ c_out,
+                                           const S* __restrict__ T_old, S* __restrict__ T_new, int zchunk, int bx,
+                                           int by, int bz, unsigned char* smem, uint32_t& par)
+{
+    using LN = Lanes<S, L>;
+    using V = typename LN::V;
+    using LY = MarchLayout<S, TY, SOL, NSLOT>;
+    constexpr int TX = 32, TW = LY::TW, NW = LY::NW, NH = LY::NH, NQ = LY::NQ, XOFF = LY::XOFF;
+    constexpr int TR = TY / L;                                    // thread rows; lane l owns row ty + l*TR
+    constexpr int ran_mode = (HEAT && !DPPW) ? 1 : ((!HEAT && DPPW) ? 2 : 0);
+    constexpr int NRING = (L == 1) ? 2 * NW + 2 * TY : NW + TY;  // ring items (pairs when L = 2)
+    static_assert(TY % L == 0, "tile height must be a multiple of the lanes");
+
+    S* const sphi = reinterpret_cast<S*>(smem);
+    const uint32_t bar0 = smem_u32(smem + LY::BAR_OFF);
+    S* const snode = reinterpret_cast<S*>(smem + LY::NODE_OFF);
+    S* const ssol = reinterpret_cast<S*>(smem + LY::SOL_OFF);
+
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    const long long px = d.px, pl = d.plane;
+    const int x0 = bx * TX, y0 = by * TY;
+    const int zb = bz * zchunk;
+    const int ze = min(zb + zchunk, nz);
+    const int zlast = min(nz - 1, ze + 1);   // the last plane any computation of this tile reads
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int tid = tx + TX * ty;
+    const bool lead = tid == 0;
+    const int x = x0 + tx;
+
+    // ---- the cells of this thread (lanes) ----
+    int yv[L];
+    bool own[L];
+    long long col[L];
+    int phi_off[L], node_off[L];
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+        yv[l] = y0 + ty + l * TR;
+        own[l] = x < nx && yv[l] < ny;
+        col[l] = (long long)x + (long long)yv[l] * px;
+        phi_off[l] = (ty + l * TR + 2) * TW + (tx + XOFF);
+        node_off[l] = (ty + l * TR + 1) * NW + (tx + 1);
+    }
+    // ---- the ring items of this thread: node-tile positions ----
+    int rlx[L], rly[L];
+    const bool ring = tid < NRING;
+    if (L == 1) {
+        int r = ring ? tid : 0;
+        if (r < NW) { rlx[0] = r; rly[0] = 0; }
+        else if ((r -= NW) < NW) { rlx[0] = r; rly[0] = NH - 1; }
+        else if ((r -= NW) < TY) { rlx[0] = 0; rly[0] = 1 + r; }
+        else { r -= TY; rlx[0] = NW - 1; rly[0] = 1 + r; }
+    } else {
+        const int r = ring ? tid : 0;
+        if (r < NW) { rlx[0] = r; rly[0] = 0; rlx[L - 1] = r; rly[L - 1] = NH - 1; }
+        else { rlx[0] = 0; rly[0] = 1 + (r - NW); rlx[L - 1] = NW - 1; rly[L - 1] = 1 + (r - NW); }
+    }
+    bool rin[L];
+    long long rcol[L];
+    int rphi_off[L], rnode_off[L];
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+        const int gx = x0 - 1 + rlx[l], gy = y0 - 1 + rly[l];
+        rin[l] = ring && gx >= 0 && gx < nx && gy >= 0 && gy < ny;
+        rcol[l] = (long long)gx + (long long)gy * px;
+        rphi_off[l] = (rly[l] + 1) * TW + (rlx[l] - 1 + XOFF);
+        rnode_off[l] = rly[l] * NW + rlx[l];
+    }
+
+    // ---- plane loads ----
+    uint32_t pend = 0;          // slots with a load issued and not yet seen complete (lead thread)
+    auto issue = [&](int p) {   // one thread: plane p into its slot
+        const int s = (p + 6) % 6;
+        const uint32_t bar = bar0 + 8 * s;
+        mbar_arrive_expect_tx(bar, (uint32_t)LY::PHI_BYTES);
+        tma_load_3d(smem_u32(sphi + s * LY::PHI_SLOT), tm, x0 - XOFF, y0 - 2, p, bar);
+        pend |= 1u << s;
+    };
+    auto wait_plane = [&](int p) -> bool {
+        const int s = (p + 6) % 6;
+        const bool ok = mbar_wait(bar0 + 8 * s, (par >> s) & 1u);
+        if (ok) {
+            par ^= 1u << s;
+            pend &= ~(1u << s);
+        }
+        return ok;
+    };
+    // after a failed wait: the lead thread waits (bounded) for the loads
+    // still in flight, so that no TMA write lands in shared memory the CTA
+    // has left
+    auto drain = [&]() {
+        if (!lead) return;
+        for (int s = 0; s < 6; ++s)
+            if ((pend >> s) & 1u) mbar_wait(bar0 + 8 * s, (par >> s) & 1u);
+    };
+
+    // node quantities of plane n into its slot, from phase planes n-1, n, n+1
+    auto node_plane = [&](int n, const S* pm, const S* p0, const S* pp) {
+        S* dst = snode + ((n + NSLOT) % NSLOT) * LY::NODE_SLOT;
+        auto one = [&](const int* off_phi, const int* off_node) {
+            S a[L], b[L];
+#pragma unroll
+            for (int l = 0; l < L; ++l) { a[l] = p0[off_phi[l] + 1]; b[l] = p0[off_phi[l] - 1]; }
+            const V gx = grad<V, true>(LN::make(a), LN::make(b), cv.dx, cv.hx);
+#pragma unroll
+            for (int l = 0; l < L; ++l) { a[l] = p0[off_phi[l] + TW]; b[l] = p0[off_phi[l] - TW]; }
+            const V gy = grad<V, true>(LN::make(a), LN::make(b), cv.dy, cv.hy);
+#pragma unroll
+            for (int l = 0; l < L; ++l) { a[l] = pp[off_phi[l]]; b[l] = pm[off_phi[l]]; }
+            const V gz = grad<V, true>(LN::make(a), LN::make(b), cv.dz, cv.hz);
+            const Node<V> q = aniso_node<V, true>(gx, gy, gz, cv);
+            const V eps2 = q.eps * q.eps;   // the stencil reads eps only squared
+#pragma unroll
+            for (int l = 0; l < L; ++l) {
+                S* o = dst + off_node[l];
+                o[0] = LN::get(eps2, l);
+                o[NQ] = LN::get(q.exy, l);
+                o[2 * NQ] = LN::get(q.eyz, l);
+                o[3 * NQ] = LN::get(q.ezx, l);
+            }
+        };
+        one(phi_off, node_off);
+        if (ring) one(rphi_off, rnode_off);
+    };
+    // solute point quantities of plane s into its slot, from phase plane s
+    // and the concentration of that plane at the own (co) and ring (cr) points
+    auto sol_plane = [&](int s, const S* p0, const S* co, const S* cr) {
+        S* dst = ssol + ((s + NSLOT) % NSLOT) * LY::SOL_SLOT;
+        auto one = [&](const int* off_phi, const int* off_node, const S* cc) {
+            S a[L];
+#pragma unroll
+            for (int l = 0; l < L; ++l) a[l] = p0[off_phi[l]];
+            const SolNode<V> q = sol_node<V, true>(LN::make(a), LN::make(cc), cv);
+#pragma unroll
+            for (int l = 0; l < L; ++l) {
+                S* o = dst + off_node[l];
+                o[0] = LN::get(q.br, l);
+                o[NQ] = LN::get(q.mu, l);
+            }
+        };
+        one(phi_off, node_off, co);
+        if (ring) one(rphi_off, rnode_off, cr);
+    };
+    // concentration of plane s at the own and ring points (a benign value
+    // outside the domain, so that no logarithm there leaves the normal range)
+    auto load_c = [&](int s, S* co, S* cr) {
+        const bool zin = s >= 0 && s < nz;
+        const long long zo = (long long)s * pl;
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+            co[l] = (zin && own[l]) ? c_in[col[l] + zo] : (S)0.02;
+            if (SOL) cr[l] = (zin && rin[l]) ? c_in[rcol[l] + zo] : (S)0.02;
+        }
+    };
+
+    // ---- the cell's flags (x / y parts; z parts are per plane) ----
+    const bool xin = x >= 1 && x <= nx - 2;    // T interior, phase source, solute interior
+    const bool xph = x >= 2 && x <= nx - 3;    // phase interior
+    const bool xone = x >= 3 && x <= nx - 4;   // sole preimage of itself
+    bool yin[L], yph[L], yone[L];
+    int xl = 0, xh = -1, yl[L], yh[L];
+    if (xin) fpre_range(x, nx, &xl, &xh);
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+        yin[l] = yv[l] >= 1 && yv[l] <= ny - 2;
+        yph[l] = yv[l] >= 2 && yv[l] <= ny - 3;
+        yone[l] = yv[l] >= 3 && yv[l] <= ny - 4;
+        yl[l] = 0;
+        yh[l] = -1;
+        if (yin[l]) fpre_range(yv[l], ny, &yl[l], &yh[l]);
+    }
+    // CTA-uniform: every column and row of the tile lies in [3, N-4]
+    const bool tile_int = x0 >= 3 && x0 + TX + 3 <= nx && y0 >= 3 && y0 + TY + 3 <= ny;
+
+    // ---- prologue: planes zb-2 .. zb+3 in flight, nodes zb-1, zb ----
+    if (lead) {
+        fence_proxy_async_smem();   // the slots may hold a previous tile's planes
+        for (int p = zb - 2; p <= zb + 3; ++p)
+            if (p >= 0 && p <= zlast) issue(p);
+    }
+    S co[3][L], cr[2][L];   // concentration: own points of planes z, z+1, z+2; ring points of z+1, z+2
+    S nd[L], nt[L];         // centre values of the next plane: DPP (or the noise), TOLD
+#pragma unroll
+    for (int l = 0; l < L; ++l) { nd[l] = 0; nt[l] = 0; cr[0][l] = cr[1][l] = 0; }
+    auto load_centre = [&](int z) {   // DPP / noise and TOLD of the own cells of plane z
+        if (!(HEAT || ran_mode == 2) || z >= ze) return;
+        const long long zo = (long long)z * pl;
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+            if (!own[l]) continue;
+            nd[l] = dpp[col[l] + zo];
+            if (HEAT) nt[l] = T_old[col[l] + zo];
+        }
+    };
+    bool bad = false;
+    if (SOL) {
+        S ca[L], cra[L];
+        load_c(zb - 1, ca, cra);
+        load_c(zb, co[0], cr[0]);
+        load_c(zb + 1, co[1], cr[1]);
+        for (int p = zb - 2; p <= zb + 1; ++p)
+            if (p >= 0 && p <= zlast) bad |= !wait_plane(p);
+        if (zb - 1 >= 0) sol_plane(zb - 1, sphi + ((zb + 5) % 6) * LY::PHI_SLOT, ca, cra);
+        sol_plane(zb, sphi + (zb % 6) * LY::PHI_SLOT, co[0], cr[0]);
+#pragma unroll
+        for (int l = 0; l < L; ++l) cr[0][l] = cr[1][l];
+    } else {
+        load_c(zb, co[0], cr[0]);
+        for (int p = zb - 2; p <= zb + 1; ++p)
+            if (p >= 0 && p <= zlast) bad |= !wait_plane(p);
+    }
+    load_centre(zb);
+    if (zb - 1 >= 1 && zb - 1 <= nz - 2)
+        node_plane(zb - 1, sphi + ((zb + 4) % 6) * LY::PHI_SLOT, sphi + ((zb + 5) % 6) * LY::PHI_SLOT,
+                   sphi + (zb % 6) * LY::PHI_SLOT);
+    if (zb >= 1 && zb <= nz - 2)
+        node_plane(zb, sphi + ((zb + 5) % 6) * LY::PHI_SLOT, sphi + (zb % 6) * LY::PHI_SLOT,
+                   sphi + ((zb + 1) % 6) * LY::PHI_SLOT);
+
+    long long zoff = (long long)zb * pl;
+    uint64_t hin[L];   // noise hash input of the own cells, carried along z (k = z + 1)
+#pragma unroll
+    for (int l = 0; l < L; ++l) hin[l] = hash_base(x + 1, yv[l] + 1, c.it, 1) + (uint64_t)(zb + 1) * kHashK;
+    int s6 = zb % 6;   // phase slot of plane z
+
+    for (int z = zb; z < ze; ++z, zoff += pl) {
+        const S* const pm = sphi + ((s6 + 5) % 6) * LY::PHI_SLOT;
+        const S* const p0 = sphi + s6 * LY::PHI_SLOT;
+        const S* const pp = sphi + ((s6 + 1) % 6) * LY::PHI_SLOT;
+        const S* const pq = sphi + ((s6 + 2) % 6) * LY::PHI_SLOT;
+        S dcur[L], tcur[L];
+#pragma unroll
+        for (int l = 0; l < L; ++l) { dcur[l] = nd[l]; tcur[l] = nt[l]; }
+        load_centre(z + 1);
+        if (SOL) load_c(z + 2, co[2], cr[1]);
+        else load_c(z + 1, co[1], cr[1]);
+
+        // A: plane z+2 has landed
+        if (z + 2 <= zlast) bad |= !wait_plane(z + 2);
+        // B, C: nodes and solute points of plane z+1
+        if (z + 1 >= 1 && z + 1 <= nz - 2) node_plane(z + 1, p0, pp, pq);
+        if (SOL && z + 1 <= nz - 1) sol_plane(z + 1, pp, co[1], cr[0]);
+        // D: one barrier orders the plane; everyone learns of a failed load
+        if (__syncthreads_or(bad)) {
+            drain();
+            return false;
+        }
+        // E: the load of plane z+4 into the slot plane z-2 has left
+        if (lead && z + 4 <= zlast) {
+            fence_proxy_async_smem();
+            issue(z + 4);
+        }
+
+        // F: the cells of plane z
+        const bool zin = z >= 1 && z <= nz - 2;   // T interior / phase source / solute interior
+        const bool zph = z >= 2 && z <= nz - 3;   // phase interior
+        const S* const nm1 = snode + ((z - 1 + NSLOT) % NSLOT) * LY::NODE_SLOT;
+        const S* const n0 = snode + (z % NSLOT) * LY::NODE_SLOT;
+        const S* const np1 = snode + ((z + 1) % NSLOT) * LY::NODE_SLOT;
+        S PPs[L];
+#pragma unroll
+        for (int l = 0; l < L; ++l) PPs[l] = p0[phi_off[l]];
+        const V PP = LN::make(PPs);
+        const V CPP = LN::make(co[0]);
+
+        // the REAL(4) noise of the own cells
+        float ran[L];
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+            if constexpr (ran_mode == 2) {
+                ran[l] = (float)dcur[l];
+            } else if constexpr (SMOOTH) {
+                ran[l] = (c.rt == 2) ? phase_ran(2, x + 1, yv[l] + 1, z + 1, c.it)
+                                     : __double2float_rn(ran64(hash63_mix(hin[l])));
+            } else {
+                ran[l] = __double2float_rn(ran64(hash63_mix(hin[l])));
+            }
+            hin[l] += kHashK;
+        }
+
+        V ppn = PP;
+        if (zph) {
+            Nbr<V> nb;
+            S t[L];
+#define PF3D_NB(FIELD, PLANE, DELTA)                                         \
+    _Pragma("unroll") for (int l = 0; l < L; ++l) t[l] = PLANE[phi_off[l] + (DELTA)]; \
+    nb.FIELD = LN::make(t);
+            nb.PP = PP;
+            PF3D_NB(PN, p0, TW) PF3D_NB(PS, p0, -TW) PF3D_NB(PE, p0, 1) PF3D_NB(PW, p0, -1)
+            PF3D_NB(PT, pp, 0) PF3D_NB(PB, pm, 0)
+            PF3D_NB(PNE, p0, TW + 1) PF3D_NB(PSE, p0, -TW + 1) PF3D_NB(PNW, p0, TW - 1) PF3D_NB(PSW, p0, -TW - 1)
+            PF3D_NB(PNT, pp, TW) PF3D_NB(PNB, pm, TW) PF3D_NB(PST, pp, -TW) PF3D_NB(PSB, pm, -TW)
+            PF3D_NB(PET, pp, 1) PF3D_NB(PEB, pm, 1) PF3D_NB(PWT, pp, -1) PF3D_NB(PWB, pm, -1)
+#undef PF3D_NB
+            Node<V> E, W, N, So, Tt, B;
+#define PF3D_ND(NODE, Q, PLANE, DELTA, QI)                                   \
+    _Pragma("unroll") for (int l = 0; l < L; ++l) t[l] = PLANE[node_off[l] + (DELTA) + (QI) * NQ]; \
+    NODE.Q = LN::make(t);
+            PF3D_ND(E, eps, n0, 1, 0) PF3D_ND(E, exy, n0, 1, 1) PF3D_ND(E, ezx, n0, 1, 3)
+            PF3D_ND(W, eps, n0, -1, 0) PF3D_ND(W, exy, n0, -1, 1) PF3D_ND(W, ezx, n0, -1, 3)
+            PF3D_ND(N, eps, n0, NW, 0) PF3D_ND(N, exy, n0, NW, 1) PF3D_ND(N, eyz, n0, NW, 2)
+            PF3D_ND(So, eps, n0, -NW, 0) PF3D_ND(So, exy, n0, -NW, 1) PF3D_ND(So, eyz, n0, -NW, 2)
+            PF3D_ND(Tt, eps, np1, 0, 0) PF3D_ND(Tt, eyz, np1, 0, 2) PF3D_ND(Tt, ezx, np1, 0, 3)
+            PF3D_ND(B, eps, nm1, 0, 0) PF3D_ND(B, eyz, nm1, 0, 2) PF3D_ND(B, ezx, nm1, 0, 3)
+#undef PF3D_ND
+            E.eyz = W.eyz = N.ezx = So.ezx = Tt.exy = B.exy = V((S)0);   // unused by the body
+            S rs[L];
+#pragma unroll
+            for (int l = 0; l < L; ++l) rs[l] = (S)ran[l];
+            ppn = phase_ppnew<V, true, true>(nb, E, W, N, So, Tt, B, CPP, LN::make(rs), cv);
+        }
+        V cn = CPP;
+        if (SOL && zin) {
+            const S* const sm1 = ssol + ((z - 1 + NSLOT) % NSLOT) * LY::SOL_SLOT;
+            const S* const s0 = ssol + (z % NSLOT) * LY::SOL_SLOT;
+            const S* const sp1 = ssol + ((z + 1) % NSLOT) * LY::SOL_SLOT;
+            SolNode<V> q[7];   // P, E, W, N, S, T, B
+            S a[L], b[L];
+#define PF3D_SN(I, PLANE, DELTA)                                                                   \
+    _Pragma("unroll") for (int l = 0; l < L; ++l) { a[l] = PLANE[node_off[l] + (DELTA)];          \
+                                                     b[l] = PLANE[node_off[l] + (DELTA) + NQ]; }  \
+    q[I].br = LN::make(a);                                                                         \
+    q[I].mu = LN::make(b);
+            PF3D_SN(0, s0, 0) PF3D_SN(1, s0, 1) PF3D_SN(2, s0, -1) PF3D_SN(3, s0, NW) PF3D_SN(4, s0, -NW)
+            PF3D_SN(5, sp1, 0) PF3D_SN(6, sm1, 0)
+#undef PF3D_SN
+            cn = conc_new<V, true>(PP, CPP, q[0], q[1], q[2], q[3], q[4], q[5], q[6], cv);
+        }
+        const V U = clamp01(ppn);
+        const V DP = ppn - PP;
+
+        if (tile_int && z >= 3 && z <= nz - 4) {
+            // every cell of the tile plane is interior and its own only
+            // preimage (CTA-uniform branch)
+#pragma unroll
+            for (int l = 0; l < L; ++l) {
+                const long long id = col[l] + zoff;
+                if (HEAT) T_new[id] = heat_at<S>(T_old, id, px, pl, PPs[l], dcur[l], c);
+                if (ran_mode == 1) dpp[id] = (S)ran[l];
+                if (DPPW) dpp[id] = LN::get(DP, l);
+                phi_out[id] = LN::get(U, l);
+                if (SOL) c_out[id] = LN::get(cn, l);
+            }
+        } else {
+#pragma unroll
+            for (int l = 0; l < L; ++l) {
+                if (!own[l]) continue;
+                const int y = yv[l];
+                const long long id = col[l] + zoff;
+                const bool src = xin && yin[l] && zin;   // T interior; phase copy source
+                if (HEAT) {
+                    S tn = tcur[l];
+                    if (src) tn = heat_at<S>(T_old, id, px, pl, PPs[l], dcur[l], c);
+                    T_new[id] = tn;
+                }
+                if (src) {
+                    const bool inner = xph && yph[l] && zph;
+                    S u = PPs[l];
+                    if (inner) {
+                        if (ran_mode == 1) dpp[id] = (S)ran[l];
+                        if (DPPW) dpp[id] = LN::get(DP, l);
+                        u = LN::get(U, l);
+                    }
+                    if (xone && yone[l] && z >= 3 && z <= nz - 4) {
+                        phi_out[id] = u;
+                    } else {
+                        int zl, zh;
+                        fpre_range(z, nz, &zl, &zh);
+                        for (int zz = zl; zz <= zh; ++zz)
+                            for (int yy = yl[l]; yy <= yh[l]; ++yy)
+                                for (int xx = xl; xx <= xh; ++xx)
+                                    phi_out[(long long)xx + (long long)yy * px + (long long)zz * pl] = u;
+                    }
+                }
+                if (SOL) {
+                    // concentracao_soluto.f90:116-124 as a fan-out: the point
+                    // writes its value to the face cells copied from it
+                    const S uc = src ? LN::get(cn, l) : co[0][l];
+                    if (src) c_out[id] = uc;
+                    if (z == 1) c_out[id - pl] = uc;
+                    if (z == nz - 2) c_out[id + pl] = uc;
+                    if (zin && x == 1) c_out[id - 1] = uc;
+                    if (zin && x == nx - 2) c_out[id + 1] = uc;
+                    if (zin && xin && y == 1) c_out[id - px] = uc;
+                    if (zin && xin && y == ny - 2) c_out[id + px] = uc;
+                }
+            }
+        }
+
+        // rotate the concentration registers and the phase slot
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+            co[0][l] = co[1][l];
+            if (SOL) {
+                co[1][l] = co[2][l];
+                cr[0][l] = cr[1][l];
+            }
+        }
+        s6 = (s6 + 1 == 6) ? 0 : s6 + 1;
+        if (NSLOT == 3) __syncthreads();   // the next plane's nodes overwrite plane z-1's slot
+    }
+    return true;
+}
+
+// resident CTAs per SM the register budget is sized for (shared memory
+// allows no more): FP64 3, or 2 for a solute pass with 4-slot windows and for
+// a pass that may draw the smooth noise (its trilinear blend of eight hashes
+// needs about 128 registers); FP32 pairs 5 for a pass with the heat
+// equation, 4 otherwise; FP32 single cells 3
+template <typename S, int L, int NSLOT, bool SOL, bool HEAT, bool SMOOTH = false>
+struct MarchOcc {
+    static constexpr int v = (sizeof(S) == 8) ? (((SOL && NSLOT == 4) || SMOOTH) ? 2 : 3)
+                                              : (L == 2 ? (HEAT ? 5 : 4) : 3);
+};
+
+// single domain: one CTA per tile; the phase field comes through `tm`
+template <typename S, int L, int TY, int NSLOT, bool HEAT, bool DPPW, bool SOL, bool SMOOTH>
+__global__ void __launch_bounds__(32 * TY / L, (MarchOcc<S, L, NSLOT, SOL, HEAT, SMOOTH>::v))
+    k_march(const __grid_constant__ CUtensorMap tm, DomainDesc d, const KC<S> c,
+            const KC<typename Lanes<S, L>::V> cv, const S* __restrict__ c_in, S* __restrict__ phi_out,
+            S* __restrict__ dpp, S* __restrict__ c_out, const S* __restrict__ T_old, S* __restrict__ T_new,
+            int zchunk, int* __restrict__ err)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char* smem = align128(smem_raw);
+    march_init_barriers<S, TY, SOL, NSLOT>(smem);
+    uint32_t par = 0;
+    if (!march_tile<S, L, TY, NSLOT, HEAT, DPPW, SOL, SMOOTH>(d, c, cv, &tm, c_in, phi_out, dpp, c_out, T_old,
+                                                                T_new, zchunk, blockIdx.x, blockIdx.y, blockIdx.z,
+                                                                smem, par)) {
+        if (threadIdx.x == 0 && threadIdx.y == 0) atomicExch(err, kErrTmaTimeout);
+    }
+}
+
+// many domains: a persistent grid walks the work list.  PASS 0 is the first
+// pass of a step (temperatura + sweep 1, or the whole step with one sweep),
+// PASS 1 the last (sweep 2 + solute).  tmaps[2 d + b] describes buffer b of
+// domain d's phase field.
+template <typename S, int L, int TY, int NSLOT, int PASS, bool ONE_SWEEP, bool SMOOTH>
+__global__ void __launch_bounds__(32 * TY / L,
+                                  (MarchOcc<S, L, NSLOT, PASS == 1 || ONE_SWEEP, PASS == 0, SMOOTH>::v))
+    k_march_batch(const BatchDomain* __restrict__ doms, const CUtensorMap* __restrict__ tmaps,
+                  const BatchStep* __restrict__ steps, const BatchItem* __restrict__ items,
+                  const int* __restrict__ n_items, int zchunk, int* __restrict__ err)
+{
+    using V = typename Lanes<S, L>::V;
+    constexpr bool SOL = PASS == 1 || ONE_SWEEP;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(16) KC<S> skc;   // the loop constants of the current item
+    __shared__ __align__(16) KC<V> skv;   // the same, broadcast to the lanes (L = 2)
+    constexpr int nf = (int)(offsetof(KC<S>, hq) / sizeof(S));
+    constexpr int NT = 32 * TY / L;
+    unsigned char* smem = align128(smem_raw);
+    march_init_barriers<S, TY, SOL, NSLOT>(smem);
+    uint32_t par = 0;
+    const int n = *n_items;
+    const int tid = threadIdx.x + 32 * threadIdx.y;
+    for (int w = blockIdx.x; w < n; w += gridDim.x) {
+        const BatchItem it = items[w];
+        const BatchStep& st = steps[it.dom];
+        if (!st.active) continue;   // uniform across the CTA
+        const BatchDomain& D = doms[it.dom];
+        const int q = st.q_phi, qc = st.q_c, qt = st.q_T;
+        __syncthreads();            // the previous item is done with the constants and the windows
+        static_assert(sizeof(KC<S>) % 4 == 0, "KC is copied as words");
+        for (int i = tid; i < (int)(sizeof(KC<S>) / 4); i += NT)
+            reinterpret_cast<int*>(&skc)[i] = reinterpret_cast<const int*>(st.kc)[i];
+        if (L == 2) {
+            __syncthreads();
+            for (int i = tid; i < nf; i += NT)
+                reinterpret_cast<V*>(&skv)[i] = V(reinterpret_cast<const S*>(&skc)[i]);
+            if (tid == 0) {
+                skv.hq = skc.hq;
+                skv.rt = skc.rt;
+                skv.it = skc.it;
+                skv.lap = skc.lap;
+            }
+        }
+        __syncthreads();
+        const KC<V>& kv = (L == 2) ? skv : *reinterpret_cast<const KC<V>*>(&skc);
+        bool ok;
+        if (PASS == 0) {
+            const CUtensorMap* tm = tmaps + 2 * it.dom + q;
+            if (ONE_SWEEP)
+                ok = march_tile<S, L, TY, NSLOT, true, true, true, SMOOTH>(
+                    D.d, skc, kv, tm, (const S*)D.c[qc], (S*)D.phi[1 - q], (S*)D.dpp, (S*)D.c[1 - qc],
+                    (const S*)D.T[qt], (S*)D.T[1 - qt], zchunk, it.bx, it.by, it.bz, smem, par);
+            else
+                ok = march_tile<S, L, TY, NSLOT, true, false, false, SMOOTH>(
+                    D.d, skc, kv, tm, (const S*)D.c[qc], (S*)D.phi[1 - q], (S*)D.dpp, nullptr, (const S*)D.T[qt],
+                    (S*)D.T[1 - qt], zchunk, it.bx, it.by, it.bz, smem, par);
+        } else {
+            const CUtensorMap* tm = tmaps + 2 * it.dom + (1 - q);
+            ok = march_tile<S, L, TY, NSLOT, false, true, true, false>(
+                D.d, skc, kv, tm, (const S*)D.c[qc], (S*)D.phi[q], (S*)D.dpp, (S*)D.c[1 - qc], nullptr, nullptr,
+                zchunk, it.bx, it.by, it.bz, smem, par);
+        }
+        if (!ok) {
+            if (tid == 0) atomicExch(err, kErrTmaTimeout);
+            return;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+
+// KC with every scalar constant broadcast to the lanes (host side)
+template <typename S, int L>
+KC<typename Lanes<S, L>::V> kc_lanes(const KC<S>& k)
+{
+    using V = typename Lanes<S, L>::V;
+    if constexpr (L == 1) {
+        return k;
+    } else {
+        KC<V> r;
+        constexpr int n = (int)(offsetof(KC<S>, hq) / sizeof(S));
+        static_assert(offsetof(KC<V>, hq) == n * sizeof(V), "KC layout");
+        const S* src = reinterpret_cast<const S*>(&k);
+        V* dst = reinterpret_cast<V*>(&r);
+        for (int i = 0; i < n; ++i) dst[i] = V::splat(src[i]);
+        r.hq = k.hq;
+        r.rt = k.rt;
+        r.it = k.it;
+        r.lap = k.lap;
+        return r;
+    }
+}
+
+template <typename S, int L, int TY, int NSLOT, bool HEAT, bool DPPW, bool SOL, bool SMOOTH>
+cudaError_t launch_march_t(const CUtensorMap& tm, const DomainDesc& d, const StepArgs& s, const void* c_in,
+                           void* phi_out, void* dpp, void* c_out, const void* T_old, void* T_new, int zchunk,
+                           int* err, cudaStream_t st)
+{
+    using LY = MarchLayout<S, TY, SOL, NSLOT>;
+    auto kern = k_march<S, L, TY, NSLOT, HEAT, DPPW, SOL, SMOOTH>;
+    static bool configured = false;   // one attribute call per instantiation
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, LY::ALLOC);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    if (zchunk <= 0) zchunk = d.nz;
+    KC<S> kc;
+    kc.load(d, s);
+    const auto kv = kc_lanes<S, L>(kc);
+    dim3 grid((d.nx + 31) / 32, (d.ny + TY - 1) / TY, (d.nz + zchunk - 1) / zchunk);
+    kern<<<grid, dim3(32, TY / L), LY::ALLOC, st>>>(tm, d, kc, kv, (const S*)c_in, (S*)phi_out, (S*)dpp, (S*)c_out,
+                                                     (const S*)T_old, (S*)T_new, zchunk, err);
+    return cudaGetLastError();
+}
+
+// the passes of a step (32 x 8 tiles).  lanes: cells per thread (1 or 2);
+// nslot: node-window planes (3 or 4).  The smooth noise runs one cell per
+// thread.
+template <typename S>
+cudaError_t launch_march_first(const CUtensorMap& tm, const DomainDesc& d, const StepArgs& s, const Fields& f,
+                               bool with_solute, int lanes, int nslot, int zchunk, int* err, cudaStream_t st)
+{
+    const bool smooth = d.rt == 2;
+#define PF3D_MF(L, NS, DW, SO, SM)                                                                            \
+    launch_march_t<S, L, 8, NS, true, DW, SO, SM>(tm, d, s, f.c_old, f.phi_mid, f.dpp, SO ? f.c_new : nullptr, \
+                                                  f.T_old, f.T_new, zchunk, err, st)
+    if (smooth) {
+        if (with_solute) return nslot == 3 ? PF3D_MF(1, 3, true, true, true) : PF3D_MF(1, 4, true, true, true);
+        return nslot == 3 ? PF3D_MF(1, 3, false, false, true) : PF3D_MF(1, 4, false, false, true);
+    }
+    if (with_solute) {
+        if (lanes == 2) return nslot == 3 ? PF3D_MF(2, 3, true, true, false) : PF3D_MF(2, 4, true, true, false);
+        return nslot == 3 ? PF3D_MF(1, 3, true, true, false) : PF3D_MF(1, 4, true, true, false);
+    }
+    if (lanes == 2) return nslot == 3 ? PF3D_MF(2, 3, false, false, false) : PF3D_MF(2, 4, false, false, false);
+    return nslot == 3 ? PF3D_MF(1, 3, false, false, false) : PF3D_MF(1, 4, false, false, false);
+#undef PF3D_MF
+}
+
+template <typename S>
+cudaError_t launch_march_last(const CUtensorMap& tm, const DomainDesc& d, const StepArgs& s, const Fields& f,
+                              int lanes, int nslot, int zchunk, int* err, cudaStream_t st)
+{
+#define PF3D_ML(L, NS)                                                                                     \
+    launch_march_t<S, L, 8, NS, false, true, true, false>(tm, d, s, f.c_old, f.phi_new, f.dpp, f.c_new, nullptr, \
+                                                          nullptr, zchunk, err, st)
+    if (lanes == 2) return nslot == 3 ? PF3D_ML(2, 3) : PF3D_ML(2, 4);
+    return nslot == 3 ? PF3D_ML(1, 3) : PF3D_ML(1, 4);
+#undef PF3D_ML
+}
+
+// The persistent grid is the SM count times the CTAs of this kernel that are
+// resident on one SM.
+template <typename S, int L, int NSLOT, int PASS, bool ONE_SWEEP, bool SMOOTH>
+cudaError_t launch_march_batch_t(const BatchDomain* doms, const CUtensorMap* tmaps, const BatchStep* steps,
+                                 const BatchItem* items, const int* n_items, int zchunk, int n_sm, int* err,
+                                 cudaStream_t st)
+{
+    constexpr bool SOL = PASS == 1 || ONE_SWEEP;
+    using LY = MarchLayout<S, 8, SOL, NSLOT>;
+    auto kern = k_march_batch<S, L, 8, NSLOT, PASS, ONE_SWEEP, SMOOTH>;
+    static int per_sm = 0;   // one attribute and occupancy query per instantiation
+    if (per_sm == 0) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, LY::ALLOC);
+        if (e != cudaSuccess) return e;
+        int nb = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 32 * 8 / L, LY::ALLOC);
+        if (e != cudaSuccess) return e;
+        per_sm = nb > 0 ? nb : 1;
+    }
+    kern<<<n_sm * per_sm, dim3(32, 8 / L), LY::ALLOC, st>>>(doms, tmaps, steps, items, n_items, zchunk, err);
+    return cudaGetLastError();
+}
+
+template <typename S>
+cudaError_t launch_march_batch(const BatchDomain* doms, const CUtensorMap* tmaps, const BatchStep* steps,
+                               const BatchItem* items, const int* n_items, int pass, bool one_sweep, bool smooth,
+                               int lanes, int nslot, int zchunk, int n_sm, int* err, cudaStream_t st)
+{
+#define PF3D_MB(L, NS, P, ONE, SM) \
+    launch_march_batch_t<S, L, NS, P, ONE, SM>(doms, tmaps, steps, items, n_items, zchunk, n_sm, err, st)
+    if (pass == 0) {
+        if (smooth) {
+            if (one_sweep) return nslot == 3 ? PF3D_MB(1, 3, 0, true, true) : PF3D_MB(1, 4, 0, true, true);
+            return nslot == 3 ? PF3D_MB(1, 3, 0, false, true) : PF3D_MB(1, 4, 0, false, true);
+        }
+        if (lanes == 2) {
+            if (one_sweep) return nslot == 3 ? PF3D_MB(2, 3, 0, true, false) : PF3D_MB(2, 4, 0, true, false);
+            return nslot == 3 ? PF3D_MB(2, 3, 0, false, false) : PF3D_MB(2, 4, 0, false, false);
+        }
+        if (one_sweep) return nslot == 3 ? PF3D_MB(1, 3, 0, true, false) : PF3D_MB(1, 4, 0, true, false);
+        return nslot == 3 ? PF3D_MB(1, 3, 0, false, false) : PF3D_MB(1, 4, 0, false, false);
+    }
+    if (lanes == 2) return nslot == 3 ? PF3D_MB(2, 3, 1, false, false) : PF3D_MB(2, 4, 1, false, false);
+    return nslot == 3 ? PF3D_MB(1, 3, 1, false, false) : PF3D_MB(1, 4, 1, false, false);
+#undef PF3D_MB
+}
+
+}  // namespace pf3d

@@ -142,7 +142,14 @@ __global__ void __launch_bounds__(256) k_copy_inner(DomainDesc d, const T* __res
 }
 
 // ---- diagnosticos.f90 + diag_body.inc ----
-// FP64 accumulation with Neumaier compensation; max/min exact.
+// FP64 accumulation with Neumaier compensation; max/min exact and NaN-
+// propagating (fmax/fmin would drop a NaN and report finite extremes for a
+// blown-up field); plus the watchdog: the count of cells whose phi or c is
+// not finite.  Partials: kDiagRow doubles per block (pf3d_launch.h).
+
+// max / min that return NaN when either argument is NaN
+__device__ __forceinline__ double nan_max(double a, double b) { return (a > b || a != a) ? a : b; }
+__device__ __forceinline__ double nan_min(double a, double b) { return (a < b || a != a) ? a : b; }
 struct KSum {
     double s, c;
     __device__ __forceinline__ void add(double v)
@@ -165,7 +172,7 @@ __global__ void __launch_bounds__(256) k_diag(DomainDesc d, const T* __restrict_
 {
     const long long ncell = (long long)d.nx * d.ny * d.nz;
     KSum l2{0, 0}, sol{0, 0}, fe{0, 0};
-    double mx = -DBL_MAX, mn = DBL_MAX;
+    double mx = -DBL_MAX, mn = DBL_MAX, bad = 0.0;
     const double dx = d.dx, dy = d.dy, dz = d.dz, E0 = d.E0, w0 = d.W0;
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
         int x = (int)(q % d.nx);
@@ -174,10 +181,12 @@ __global__ void __launch_bounds__(256) k_diag(DomainDesc d, const T* __restrict_
         int z = (int)(r / d.ny);
         long long id = cell_off(d, x, y, z);
         double phi = (double)pn[id];
+        const double cv = (double)cn[id];
         l2.add(phi * phi);
-        mx = fmax(mx, phi);
-        mn = fmin(mn, phi);
-        sol.add((double)cn[id]);
+        mx = nan_max(mx, phi);
+        mn = nan_min(mn, phi);
+        sol.add(cv);
+        if (!isfinite(phi) || !isfinite(cv)) bad += 1.0;
         double w_term = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(w0, phi), phi), 1.0 - phi), 1.0 - phi);
         double grad2 = 0.0;
         if (x > 0 && x < d.nx - 1 && y > 0 && y < d.ny - 1 && z > 0 && z < d.nz - 1) {
@@ -189,31 +198,33 @@ __global__ void __launch_bounds__(256) k_diag(DomainDesc d, const T* __restrict_
         double e = __dadd_rn(__dmul_rn(__dmul_rn(__dmul_rn(0.5, E0), E0), grad2), w_term);
         fe.add(__dmul_rn(__dmul_rn(__dmul_rn(e, dx), dy), dz));
     }
-    __shared__ double sh[8][8];
-    double v[8] = {l2.s, l2.c, mx, mn, sol.s, sol.c, fe.s, fe.c};
+    __shared__ double sh[8][9];
+    double v[9] = {l2.s, l2.c, mx, mn, sol.s, sol.c, fe.s, fe.c, bad};
     // warp reduction (fixed order, deterministic for a fixed launch shape)
     for (int off = 16; off > 0; off >>= 1) {
-        double o[8];
-        for (int q = 0; q < 8; ++q) o[q] = __shfl_down_sync(0xffffffffu, v[q], off);
+        double o[9];
+        for (int q = 0; q < 9; ++q) o[q] = __shfl_down_sync(0xffffffffu, v[q], off);
         KSum a{v[0], v[1]}; a.merge(o[0], o[1]); v[0] = a.s; v[1] = a.c;
-        v[2] = fmax(v[2], o[2]); v[3] = fmin(v[3], o[3]);
+        v[2] = nan_max(v[2], o[2]); v[3] = nan_min(v[3], o[3]);
         KSum b{v[4], v[5]}; b.merge(o[4], o[5]); v[4] = b.s; v[5] = b.c;
         KSum e{v[6], v[7]}; e.merge(o[6], o[7]); v[6] = e.s; v[7] = e.c;
+        v[8] += o[8];
     }
     int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     if (l == 0)
-        for (int q = 0; q < 8; ++q) sh[w][q] = v[q];
+        for (int q = 0; q < 9; ++q) sh[w][q] = v[q];
     __syncthreads();
     if (threadIdx.x == 0) {
         int nw = blockDim.x >> 5;
-        for (int q = 0; q < 8; ++q) v[q] = sh[0][q];
+        for (int q = 0; q < 9; ++q) v[q] = sh[0][q];
         for (int ww = 1; ww < nw; ++ww) {
             KSum a{v[0], v[1]}; a.merge(sh[ww][0], sh[ww][1]); v[0] = a.s; v[1] = a.c;
-            v[2] = fmax(v[2], sh[ww][2]); v[3] = fmin(v[3], sh[ww][3]);
+            v[2] = nan_max(v[2], sh[ww][2]); v[3] = nan_min(v[3], sh[ww][3]);
             KSum b{v[4], v[5]}; b.merge(sh[ww][4], sh[ww][5]); v[4] = b.s; v[5] = b.c;
             KSum e{v[6], v[7]}; e.merge(sh[ww][6], sh[ww][7]); v[6] = e.s; v[7] = e.c;
+            v[8] += sh[ww][8];
         }
-        for (int q = 0; q < 8; ++q) part[(long long)blockIdx.x * 8 + q] = v[q];
+        for (int q = 0; q < 9; ++q) part[(long long)blockIdx.x * kDiagRow + q] = v[q];
     }
 }
 
@@ -222,20 +233,22 @@ __global__ void k_diag_final(const double* __restrict__ part, int nblk, double* 
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     KSum l2{0, 0}, sol{0, 0}, fe{0, 0};
-    double mx = -DBL_MAX, mn = DBL_MAX;
+    double mx = -DBL_MAX, mn = DBL_MAX, bad = 0.0;
     for (int b = 0; b < nblk; ++b) {
-        const double* p = part + (long long)b * 8;
+        const double* p = part + (long long)b * kDiagRow;
         l2.merge(p[0], p[1]);
-        mx = fmax(mx, p[2]);
-        mn = fmin(mn, p[3]);
+        mx = nan_max(mx, p[2]);
+        mn = nan_min(mn, p[3]);
         sol.merge(p[4], p[5]);
         fe.merge(p[6], p[7]);
+        bad += p[8];
     }
     out[0] = sqrt(l2.s + l2.c);
     out[1] = mx;
     out[2] = mn;
     out[3] = sol.s + sol.c;
     out[4] = fe.s + fe.c;
+    out[5] = bad;   // cells with a non-finite phi or c (the watchdog)
 }
 
 // ---- host conversion staging (FP32 contexts) ----

@@ -19,7 +19,7 @@ from . import _abi
 from ._abi import (LIB, check, pf_grid, pf_params, pf_derived, pf_state, PFError,
                    PF_FP64, PF_FP32, PF_PHASE_OLD, PF_PHASE_NEW, PF_CONC_OLD, PF_CONC_NEW,
                    PF_TOLD, PF_TNEW, PF_DPP, PF_OPT_FUSED, PF_OPT_TILE_Y, PF_OPT_ZCHUNK,
-                   PF_OPT_KTIMING, PF_OPT_PAIRED, FIELD_NAMES)
+                   PF_OPT_KTIMING, PF_OPT_PAIRED, PF_OPT_KERNEL, PF_OPT_NSLOT, PF_E_KERNEL, PF_E_NONFINITE, FIELD_NAMES)
 from .deck import run6_params, params_copy, grid, read_entrada, WORKLOADS, Workload
 
 __all__ = ["Domain", "PFError", "run6_params", "params_copy", "grid", "read_entrada", "WORKLOADS", "Workload",
@@ -262,6 +262,7 @@ class Batch:
         check(LIB.pf_batch_create(precision, int(budget_bytes), int(max_domains), C.byref(h)))
         self._h = h
         self.precision = precision
+        self._max = int(max_domains)
         self.grids = {}
 
     def close(self):
@@ -328,6 +329,12 @@ class Batch:
     def set_target(self, slot: int, target_it: int):
         self._chk(LIB.pf_batch_set_target(self._h, slot, int(target_it)))
 
+    def progress(self) -> np.ndarray:
+        """Step count of every slot (-1 for a free slot), one library call."""
+        it = np.empty(self._max, dtype=np.int32)
+        self._chk(LIB.pf_batch_progress(self._h, it.ctypes.data_as(C.POINTER(C.c_int)), self._max))
+        return it
+
     def state(self, slot: int) -> pf_state:
         st = pf_state()
         self._chk(LIB.pf_batch_get_state(self._h, slot, C.byref(st)))
@@ -352,6 +359,10 @@ class Batch:
 
     def set_paired(self, paired: int):
         self._chk(LIB.pf_batch_set_paired(self._h, int(paired)))
+
+    def set_kernel(self, kernel: int, nslot: int = 0):
+        """1: the TMA-staged passes (default), 0: the cp.async passes."""
+        self._chk(LIB.pf_batch_set_kernel(self._h, int(kernel), int(nslot)))
 
     def autotune(self, steps_per_candidate: int = 2):
         ty, zc, ms = C.c_int(), C.c_int(), C.c_double()

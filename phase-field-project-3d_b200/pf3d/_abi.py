@@ -13,12 +13,13 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libpf3d.so")
 
-PF_OK, PF_E_ARG, PF_E_CUDA, PF_E_NOMEM, PF_E_STATE, PF_E_NODEV = 0, -1, -2, -3, -4, -5
+PF_OK, PF_E_ARG, PF_E_CUDA, PF_E_NOMEM, PF_E_STATE, PF_E_NODEV, PF_E_KERNEL, PF_E_NONFINITE = (
+    0, -1, -2, -3, -4, -5, -6, -7)
 PF_PHASE_OLD, PF_PHASE_NEW, PF_CONC_OLD, PF_CONC_NEW, PF_TOLD, PF_TNEW, PF_DPP = range(7)
 FIELD_NAMES = ("phase_field_old", "phase_field_new", "conc_soluto_old", "conc_soluto_new", "TOLD", "TNEW", "DPP")
 PF_FP64, PF_FP32 = 64, 32
 PF_BC_REFERENCE = 0
-PF_OPT_FUSED, PF_OPT_TILE_Y, PF_OPT_ZCHUNK, PF_OPT_KTIMING, PF_OPT_PAIRED = 1, 2, 3, 4, 5
+PF_OPT_FUSED, PF_OPT_TILE_Y, PF_OPT_ZCHUNK, PF_OPT_KTIMING, PF_OPT_PAIRED, PF_OPT_KERNEL, PF_OPT_NSLOT = 1, 2, 3, 4, 5, 6, 7
 PF_NOALLOC_MAX_PLANES = 4096
 
 
@@ -114,12 +115,14 @@ SIGNATURES = [
     ("pf_batch_init_seeded", C.c_int, [_P, C.c_int, C.c_int, _D]),
     ("pf_batch_set_target", C.c_int, [_P, C.c_int, C.c_longlong]),
     ("pf_batch_get_state", C.c_int, [_P, C.c_int, C.POINTER(pf_state)]),
+    ("pf_batch_progress", C.c_int, [_P, _I, C.c_int]),
     ("pf_batch_step", C.c_int, [_P, C.c_int]),
     ("pf_batch_step_async", C.c_int, [_P, C.c_int]),
     ("pf_batch_wait", C.c_int, [_P]),
     ("pf_batch_last_ms", C.c_double, [_P]),
     ("pf_batch_set_tile", C.c_int, [_P, C.c_int, C.c_int]),
     ("pf_batch_set_paired", C.c_int, [_P, C.c_int]),
+    ("pf_batch_set_kernel", C.c_int, [_P, C.c_int, C.c_int]),
     ("pf_batch_autotune", C.c_int, [_P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _D]),
     ("pf_batch_diagnosticos", C.c_int, [_P, C.c_int, _D]),
     ("pf_batch_track", C.c_int, [_P, C.c_int, _D]),

@@ -18,8 +18,11 @@ precisions running at the same time on their own streams), and a request
 retires -- its diagnostics and its solid fraction and tip position
 (evaluated on the device) read back, its memory freed -- as soon as it has
 done its steps, which lets the next waiting requests in.  No field ever
-leaves the device.  Latency of a
-request = completion time - arrival time.
+leaves the device.  Latency of a request = completion time - arrival time;
+its admission wait = admission time - arrival time.  The loop polls the
+progress of a whole batch in one library call per quantum.  A request whose
+state has gone non-finite (the diagnostics' watchdog, PF_E_NONFINITE) is
+retired as failed, without numbers.
 """
 from __future__ import annotations
 
@@ -30,7 +33,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import Batch, PF_FP32, PF_FP64, _abi
+from . import Batch, PF_FP32, PF_FP64, PFError, _abi
 from .deck import grid, run6_params
 from .init import bump_sites
 
@@ -57,6 +60,7 @@ class Job:
     slot: int = -1
     result: tuple = ()      # diagnostics of the final state (pf_batch_diagnosticos)
     track: tuple = ()       # solid fraction, tip position, solid cells (pf_batch_track)
+    failed: bool = False    # the state went non-finite (retired without numbers)
 
     @property
     def cells(self) -> int:
@@ -146,12 +150,20 @@ class Server:
         self.active[job.precision][slot] = job
         return True
 
-    def _retire(self, now: float, done: list):
+    def _retire(self, now: float, done: list, progress: dict):
         for prec, b in self.batches.items():
+            it = progress.get(prec)
             for slot, job in list(self.active[prec].items()):
-                if b.state(slot).it >= job.steps:
-                    job.result = b.diagnosticos(slot)
-                    job.track = b.track(slot)
+                if it is not None and it[slot] >= job.steps:
+                    try:
+                        job.result = b.diagnosticos(slot)
+                        job.track = b.track(slot)
+                    except PFError as e:
+                        if e.code != _abi.PF_E_NONFINITE:
+                            raise
+                        job.failed = True
+                        job.result = ()
+                        job.track = ()
                     job.done = now
                     b.remove(slot)
                     self.used -= self.bytes_of(job)
@@ -166,6 +178,8 @@ class Server:
         nxt = 0
         t0 = clock()
         device_ms = 0.0
+        peak_used = 0
+        waited_for_memory = 0
         while len(done) < len(jobs):
             now = clock() - t0
             while nxt < len(jobs) and jobs[nxt].arrival <= now:
@@ -174,6 +188,9 @@ class Server:
             # FIFO admission while the head fits the budget
             while waiting and self._admit(waiting[0], now):
                 waiting.pop(0)
+            if waiting:
+                waited_for_memory = max(waited_for_memory, len(waiting))
+            peak_used = max(peak_used, self.used)
             if not any(self.active.values()):
                 if nxt < len(jobs):
                     time.sleep(max(0.0, min(0.01, jobs[nxt].arrival - (clock() - t0))))
@@ -184,19 +201,28 @@ class Server:
             stepped = []
             for prec, b in self.batches.items():
                 if self.active[prec]:
-                    before = {s: b.state(s).it for s in self.active[prec]}
+                    before = b.progress()
                     b.step_async(self.quantum)
                     stepped.append((prec, b, before))
+            progress = {}
             for prec, b, before in stepped:
                 device_ms += b.wait()
-                self.gcell_updates += sum(self.active[prec][s].cells * (b.state(s).it - before[s])
-                                          for s in self.active[prec]) / 1e9
-            self._retire(clock() - t0, done)
+                after = b.progress()
+                progress[prec] = after
+                self.gcell_updates += sum(job.cells * int(after[s] - before[s])
+                                          for s, job in self.active[prec].items()) / 1e9
+            self._retire(clock() - t0, done, progress)
             if on_quantum:
                 on_quantum(self, done, waiting)
         wall = clock() - t0
         lat = np.array([j.done - j.arrival for j in done])
-        return {"requests": len(done), "wall_s": wall, "device_ms": device_ms,
-                "gcell_updates": self.gcell_updates, "gcell_per_s": self.gcell_updates / wall,
+        adm = np.array([j.admitted - j.arrival for j in done])
+        return {"requests": len(done), "failed": sum(1 for j in done if j.failed), "wall_s": wall,
+                "device_ms": device_ms, "gcell_updates": self.gcell_updates,
+                "gcell_per_s": self.gcell_updates / wall,
                 "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-                "mean_s": float(lat.mean())}
+                "mean_s": float(lat.mean()),
+                "admission_wait_p50_s": float(np.percentile(adm, 50)),
+                "admission_wait_p99_s": float(np.percentile(adm, 99)),
+                "peak_budget_used_gb": peak_used / 1e9, "budget_gb": self.budget / 1e9,
+                "max_waiting_for_memory": waited_for_memory}

@@ -9,7 +9,7 @@ import types
 
 import pytest
 
-from pf3d import PF_FP32, PF_FP64
+from pf3d import PF_FP32, PF_FP64, PFError, PF_E_NONFINITE
 from pf3d.serve import Job, Server
 
 
@@ -38,6 +38,9 @@ class FakeBatch:
     def state(self, slot):
         return types.SimpleNamespace(it=self.slots[slot]["it"])
 
+    def progress(self):
+        return {s: st["it"] for s, st in self.slots.items()}
+
     def step_async(self, n):
         FakeBatch.log.append(("step", self.precision))
         self.pending = n
@@ -49,8 +52,12 @@ class FakeBatch:
         self.pending = 0
         return 1.0
 
+    blown = set()   # (precision, slot) whose state the watchdog finds non-finite
+
     def diagnosticos(self, slot):
         assert self.slots[slot]["seeded"]
+        if (self.precision, slot) in FakeBatch.blown:
+            raise PFError(PF_E_NONFINITE, "cells hold a non-finite phi or c")
         return (1.0, 1.0, 0.0, 2.0, 3.0)
 
     def track(self, slot):
@@ -115,3 +122,33 @@ def test_request_larger_than_the_budget_is_an_error():
     srv = Server(budget_bytes=10, quantum=8, batch_factory=FakeBatch, bytes_of=lambda j: 11)
     with pytest.raises(RuntimeError, match="does not fit"):
         srv.run([_job(0, 8, PF_FP32, 0.0)], clock=Clock(0.01))
+
+
+def test_admission_wait_and_budget_use_are_reported():
+    FakeBatch.log.clear()
+    FakeBatch.blown.clear()
+    jobs = [_job(0, 40, PF_FP32, 0.0), _job(1, 16, PF_FP32, 0.0), _job(2, 8, PF_FP32, 0.0)]
+    srv = Server(budget_bytes=100, quantum=8, batch_factory=FakeBatch, bytes_of=lambda j: 60)
+    out = srv.run(jobs, clock=Clock(0.01))
+    assert out["requests"] == 3 and out["failed"] == 0
+    # one request fits at a time: the others wait for memory
+    assert out["max_waiting_for_memory"] == 2
+    assert out["peak_budget_used_gb"] == pytest.approx(60 / 1e9)
+    assert out["admission_wait_p99_s"] >= out["admission_wait_p50_s"] > 0
+    j = {x.jid: x for x in jobs}
+    assert j[1].admitted >= j[0].done and j[2].admitted >= j[1].done
+
+
+def test_a_blown_up_request_retires_as_failed():
+    FakeBatch.log.clear()
+    FakeBatch.blown.clear()
+    jobs = [_job(0, 16, PF_FP32, 0.0), _job(1, 16, PF_FP32, 0.0), _job(2, 16, PF_FP64, 0.0)]
+    srv = Server(budget_bytes=1000, quantum=8, batch_factory=FakeBatch, bytes_of=lambda j: 10)
+    FakeBatch.blown.add((PF_FP32, 1))   # the second FP32 slot (job 1)
+    out = srv.run(jobs, clock=Clock(0.01))
+    FakeBatch.blown.clear()
+    assert out["requests"] == 3 and out["failed"] == 1
+    j = {x.jid: x for x in jobs}
+    assert j[1].failed and j[1].result == () and j[1].track == ()
+    assert not j[0].failed and j[0].result == (1.0, 1.0, 0.0, 2.0, 3.0)
+    assert srv.used == 0 and all(not b.slots for b in srv.batches.values())
