@@ -153,10 +153,12 @@ int pf_set_stream(pf_ctx* ctx, void* stream);
                               plane loads on mbarriers, uniform per-cell
                               arithmetic with fan-out boundary stores; 0 the
                               element-wise cp.async passes.  Same results.  */
-#define PF_OPT_NSLOT 7     /* node-window planes of the TMA passes: 3 (two
-                              barriers a plane, less shared memory) or 4
-                              (one barrier); 0 (default) = 3 in FP64, 4 in
-                              FP32                                          */
+#define PF_OPT_NSLOT 7     /* window mode of the TMA passes: 3 (3-plane
+                              node windows, two barriers a plane), 4 (4-plane
+                              windows, one barrier) or 5 (the own column's
+                              values carried in registers along z, 3-plane
+                              windows, one barrier); 0 (default) = the
+                              precision's measured best.  Same results.     */
 int pf_set_option(pf_ctx* ctx, int opt, int value);
 int pf_get_option(const pf_ctx* ctx, int opt, int* value);
 /* With PF_OPT_KTIMING on: launches and summed device milliseconds of the

@@ -289,7 +289,8 @@ int pf_set_option(pf_ctx* ctx, int opt, int value)
         ctx->kernel = value;
         return PF_OK;
     case PF_OPT_NSLOT:
-        if (value != 0 && value != 3 && value != 4) return ctx_err(ctx, PF_E_ARG, "nslot must be 0, 3 or 4");
+        if (value != 0 && value != 3 && value != 4 && value != 5)
+            return ctx_err(ctx, PF_E_ARG, "window mode must be 0, 3, 4 or 5");
         ctx->nslot = value;
         return PF_OK;
     }

@@ -618,8 +618,8 @@ int pf_batch_set_paired(pf_batch* b, int paired)
 
 int pf_batch_set_kernel(pf_batch* b, int kernel, int nslot)
 {
-    if (!b || kernel < 0 || kernel > 1 || (nslot != 0 && nslot != 3 && nslot != 4))
-        return berr(b, PF_E_ARG, "pf_batch_set_kernel: kernel 0 or 1, nslot 0, 3 or 4");
+    if (!b || kernel < 0 || kernel > 1 || (nslot != 0 && nslot != 3 && nslot != 4 && nslot != 5))
+        return berr(b, PF_E_ARG, "pf_batch_set_kernel: kernel 0 or 1, window mode 0, 3, 4 or 5");
     if (kernel == 1 && !tmap_encoder())
         return berr(b, PF_E_STATE, "pf_batch_set_kernel: this driver has no tensor-map encoder");
     if (kernel == 1 && !b->march) {

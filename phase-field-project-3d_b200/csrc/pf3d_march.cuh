@@ -13,9 +13,9 @@
 //    the context's status word and the CTA stops (pf3d_tma.cuh).
 //  * Node windows.  The anisotropy quantities (eps^2, exy, eyz, ezx) of every
 //    node of the tile and its 1-cell ring, and the solute point quantities
-//    (Gamma bracket, mu), are computed once per plane into NSLOT-plane
-//    windows.  With NSLOT = 4 one barrier per plane orders everything; with
-//    NSLOT = 3 (less shared memory) a second barrier closes each plane.
+//    (Gamma bracket, mu), are computed once per plane into 3- or 4-plane
+//    windows; the window mode (MarchWin) says how many and how many barriers
+//    a plane takes, and whether the own column's values roll in registers.
 //  * Uniform arithmetic, fan-out stores.  Every cell of every tile -- also
 //    the tiles on the domain boundary -- goes through the same arithmetic
 //    (two cells per thread as lane pairs when L = 2, packed f32x2 in FP32).
@@ -49,6 +49,23 @@ template <typename S> struct Lanes<S, 2> {
     using V = typename PairOf<S>::type;
     static __device__ __forceinline__ V make(const S* a) { return V(a[0], a[1]); }
     static __device__ __forceinline__ S get(const V& v, int l) { return l ? v.y() : v.x(); }
+};
+
+// Window modes of the march passes:
+//   3: node / solute-point windows of 3 planes, two barriers per plane;
+//   4: windows of 4 planes, one barrier per plane;
+//   5: the own column's values rolled in registers along z -- the phase
+//      values of planes z-1, z, z+1 at the cell and its four axis
+//      neighbours, the cell's node quantities of planes z-1, z, z+1 and its
+//      solute-point quantities of the same planes -- so the stencil reads
+//      from shared memory only the in-plane neighbours of plane z (the
+//      diagonal phase values and the four neighbour nodes and points);
+//      windows of 3 planes then need one barrier per plane.
+template <int WIN> struct MarchWin {
+    static_assert(WIN == 3 || WIN == 4 || WIN == 5, "window mode 3, 4 or 5");
+    static constexpr int nslot = (WIN == 4) ? 4 : 3;
+    static constexpr bool roll = WIN == 5;
+    static constexpr bool two_barriers = WIN == 3;
 };
 
 // Shared-memory layout of one tile (bytes from a 128-byte aligned base).
@@ -113,7 +130,7 @@ __device__ __forceinline__ void march_init_barriers(unsigned char* smem)
 // parity of each plane barrier across the tiles a CTA processes (every load
 // issued is waited for).  Returns false if a plane load did not arrive in
 // time; the CTA must then stop.
-template <typename S, int L, int TY, int NSLOT, bool HEAT, bool DPPW, bool SOL, bool SMOOTH>
+template <typename S, int L, int TY, int WIN, bool HEAT, bool DPPW, bool SOL, bool SMOOTH>
 __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, const KC<typename Lanes<S, L>::V>& cv,
                                            const CUtensorMap* tm, const S* __restrict__ c_in,
                                            S* __restrict__ phi_out, S* __restrict__ dpp, S* __restrict__ c_out,
@@ -122,6 +139,8 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
 {
     using LN = Lanes<S, L>;
     using V = typename LN::V;
+    constexpr int NSLOT = MarchWin<WIN>::nslot;
+    constexpr bool ROLL = MarchWin<WIN>::roll;
     using LY = MarchLayout<S, TY, SOL, NSLOT>;
     constexpr int TX = 32, TW = LY::TW, NW = LY::NW, NH = LY::NH, NQ = LY::NQ, XOFF = LY::XOFF;
     constexpr int TR = TY / L;                                    // thread rows; lane l owns row ty + l*TR
@@ -211,10 +230,30 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
             if ((pend >> s) & 1u) mbar_wait(bar0 + 8 * s, (par >> s) & 1u);
     };
 
+    // the node quantities of one set of items from their gradient; stored
+    // into the slot `dst`; the own items' eps^2, eyz, ezx also into `keep`
+    auto node_store = [&](S* dst, const int* off_node, V gx, V gy, V gz, S (*keep)[3]) {
+        const Node<V> q = aniso_node<V, true>(gx, gy, gz, cv);
+        const V eps2 = q.eps * q.eps;   // the stencil reads eps only squared
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+            S* o = dst + off_node[l];
+            o[0] = LN::get(eps2, l);
+            o[NQ] = LN::get(q.exy, l);
+            o[2 * NQ] = LN::get(q.eyz, l);
+            o[3 * NQ] = LN::get(q.ezx, l);
+            if (keep) {
+                keep[l][0] = LN::get(eps2, l);
+                keep[l][1] = LN::get(q.eyz, l);
+                keep[l][2] = LN::get(q.ezx, l);
+            }
+        }
+    };
     // node quantities of plane n into its slot, from phase planes n-1, n, n+1
-    auto node_plane = [&](int n, const S* pm, const S* p0, const S* pp) {
+    // in shared memory (own items' values also into `keep` when given)
+    auto node_plane = [&](int n, const S* pm, const S* p0, const S* pp, S (*keep)[3]) {
         S* dst = snode + ((n + NSLOT) % NSLOT) * LY::NODE_SLOT;
-        auto one = [&](const int* off_phi, const int* off_node) {
+        auto one = [&](const int* off_phi, const int* off_node, S (*kp)[3]) {
             S a[L], b[L];
 #pragma unroll
             for (int l = 0; l < L; ++l) { a[l] = p0[off_phi[l] + 1]; b[l] = p0[off_phi[l] - 1]; }
@@ -225,38 +264,35 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
 #pragma unroll
             for (int l = 0; l < L; ++l) { a[l] = pp[off_phi[l]]; b[l] = pm[off_phi[l]]; }
             const V gz = grad<V, true>(LN::make(a), LN::make(b), cv.dz, cv.hz);
-            const Node<V> q = aniso_node<V, true>(gx, gy, gz, cv);
-            const V eps2 = q.eps * q.eps;   // the stencil reads eps only squared
-#pragma unroll
-            for (int l = 0; l < L; ++l) {
-                S* o = dst + off_node[l];
-                o[0] = LN::get(eps2, l);
-                o[NQ] = LN::get(q.exy, l);
-                o[2 * NQ] = LN::get(q.eyz, l);
-                o[3 * NQ] = LN::get(q.ezx, l);
-            }
+            node_store(dst, off_node, gx, gy, gz, kp);
         };
-        one(phi_off, node_off);
-        if (ring) one(rphi_off, rnode_off);
+        one(phi_off, node_off, keep);
+        if (ring) one(rphi_off, rnode_off, nullptr);
     };
     // solute point quantities of plane s into its slot, from phase plane s
-    // and the concentration of that plane at the own (co) and ring (cr) points
-    auto sol_plane = [&](int s, const S* p0, const S* co, const S* cr) {
+    // and the concentration of that plane at the own (co) and ring (cr)
+    // points; the own points' values also into `keep` when given, and their
+    // phase values taken from `ownp` when given
+    auto sol_plane = [&](int s, const S* p0, const S* co, const S* cr, S (*keep)[2], const S* ownp) {
         S* dst = ssol + ((s + NSLOT) % NSLOT) * LY::SOL_SLOT;
-        auto one = [&](const int* off_phi, const int* off_node, const S* cc) {
+        auto one = [&](const int* off_phi, const int* off_node, const S* cc, S (*kp)[2], const S* op) {
             S a[L];
 #pragma unroll
-            for (int l = 0; l < L; ++l) a[l] = p0[off_phi[l]];
+            for (int l = 0; l < L; ++l) a[l] = op ? op[l] : p0[off_phi[l]];
             const SolNode<V> q = sol_node<V, true>(LN::make(a), LN::make(cc), cv);
 #pragma unroll
             for (int l = 0; l < L; ++l) {
                 S* o = dst + off_node[l];
                 o[0] = LN::get(q.br, l);
                 o[NQ] = LN::get(q.mu, l);
+                if (kp) {
+                    kp[l][0] = LN::get(q.br, l);
+                    kp[l][1] = LN::get(q.mu, l);
+                }
             }
         };
-        one(phi_off, node_off, co);
-        if (ring) one(rphi_off, rnode_off, cr);
+        one(phi_off, node_off, co, keep, ownp);
+        if (ring) one(rphi_off, rnode_off, cr, nullptr, nullptr);
     };
     // concentration of plane s at the own and ring points (a benign value
     // outside the domain, so that no logarithm there leaves the normal range)
@@ -299,14 +335,35 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
     S nd[L], nt[L];         // centre values of the next plane: DPP (or the noise), TOLD
 #pragma unroll
     for (int l = 0; l < L; ++l) { nd[l] = 0; nt[l] = 0; cr[0][l] = cr[1][l] = 0; }
-    auto load_centre = [&](int z) {   // DPP / noise and TOLD of the own cells of plane z
+    // DPP / noise and TOLD of the own cells of plane z.  TOLD is read only
+    // where the heat equation keeps it (outside 2..N-1): inside, TNEW is TP
+    // plus the latent term (and the Laplacian reads its own neighbours)
+    auto load_centre = [&](int z) {
         if (!(HEAT || ran_mode == 2) || z >= ze) return;
         const long long zo = (long long)z * pl;
+        const bool zi = z >= 1 && z <= nz - 2;
 #pragma unroll
         for (int l = 0; l < L; ++l) {
             if (!own[l]) continue;
             nd[l] = dpp[col[l] + zo];
-            if (HEAT) nt[l] = T_old[col[l] + zo];
+            if (HEAT && !(zi && x >= 1 && x <= nx - 2 && yv[l] >= 1 && yv[l] <= ny - 2)) nt[l] = T_old[col[l] + zo];
+        }
+    };
+    // rolled own-column state (window mode 5): phase values of planes z-1,
+    // z, z+1 at the cell and its N, S, E, W neighbours; the cell's node
+    // (eps^2, eyz, ezx) and solute-point (bracket, mu) quantities of the same
+    // planes.  Index of the five phase values: cell, N, S, E, W.  Unused, and
+    // so not allocated, in the other modes.
+    S rpm[L][5], rp0[L][5], rpp[L][5];
+    S rnB[L][3], rnC[L][3], rnT[L][3];
+    S rsB[L][2], rsP[L][2], rsT[L][2];
+    auto load5 = [&](S (*dst)[5], const S* pl_) {
+        if constexpr (ROLL) {
+#pragma unroll
+            for (int l = 0; l < L; ++l) {
+                const S* q = pl_ + phi_off[l];
+                dst[l][0] = q[0]; dst[l][1] = q[TW]; dst[l][2] = q[-TW]; dst[l][3] = q[1]; dst[l][4] = q[-1];
+            }
         }
     };
     bool bad = false;
@@ -317,8 +374,8 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
         load_c(zb + 1, co[1], cr[1]);
         for (int p = zb - 2; p <= zb + 1; ++p)
             if (p >= 0 && p <= zlast) bad |= !wait_plane(p);
-        if (zb - 1 >= 0) sol_plane(zb - 1, sphi + ((zb + 5) % 6) * LY::PHI_SLOT, ca, cra);
-        sol_plane(zb, sphi + (zb % 6) * LY::PHI_SLOT, co[0], cr[0]);
+        if (zb - 1 >= 0) sol_plane(zb - 1, sphi + ((zb + 5) % 6) * LY::PHI_SLOT, ca, cra, ROLL ? rsB : nullptr, nullptr);
+        sol_plane(zb, sphi + (zb % 6) * LY::PHI_SLOT, co[0], cr[0], ROLL ? rsP : nullptr, nullptr);
 #pragma unroll
         for (int l = 0; l < L; ++l) cr[0][l] = cr[1][l];
     } else {
@@ -329,10 +386,12 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
     load_centre(zb);
     if (zb - 1 >= 1 && zb - 1 <= nz - 2)
         node_plane(zb - 1, sphi + ((zb + 4) % 6) * LY::PHI_SLOT, sphi + ((zb + 5) % 6) * LY::PHI_SLOT,
-                   sphi + (zb % 6) * LY::PHI_SLOT);
+                   sphi + (zb % 6) * LY::PHI_SLOT, ROLL ? rnB : nullptr);
     if (zb >= 1 && zb <= nz - 2)
         node_plane(zb, sphi + ((zb + 5) % 6) * LY::PHI_SLOT, sphi + (zb % 6) * LY::PHI_SLOT,
-                   sphi + ((zb + 1) % 6) * LY::PHI_SLOT);
+                   sphi + ((zb + 1) % 6) * LY::PHI_SLOT, ROLL ? rnC : nullptr);
+    load5(rpm, sphi + ((zb + 5) % 6) * LY::PHI_SLOT);
+    load5(rp0, sphi + (zb % 6) * LY::PHI_SLOT);
 
     long long zoff = (long long)zb * pl;
     uint64_t hin[L];   // noise hash input of the own cells, carried along z (k = z + 1)
@@ -355,8 +414,44 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
         // A: plane z+2 has landed
         if (z + 2 <= zlast) bad |= !wait_plane(z + 2);
         // B, C: nodes and solute points of plane z+1
-        if (z + 1 >= 1 && z + 1 <= nz - 2) node_plane(z + 1, p0, pp, pq);
-        if (SOL && z + 1 <= nz - 1) sol_plane(z + 1, pp, co[1], cr[0]);
+        if constexpr (ROLL) {
+            load5(rpp, pp);   // plane z+1 at the own column: the stencil's T values and the node's x/y gradient
+            if (z + 1 >= 1 && z + 1 <= nz - 2) {
+                S a[L], b[L];
+#pragma unroll
+                for (int l = 0; l < L; ++l) { a[l] = rpp[l][3]; b[l] = rpp[l][4]; }
+                const V gx = grad<V, true>(LN::make(a), LN::make(b), cv.dx, cv.hx);
+#pragma unroll
+                for (int l = 0; l < L; ++l) { a[l] = rpp[l][1]; b[l] = rpp[l][2]; }
+                const V gy = grad<V, true>(LN::make(a), LN::make(b), cv.dy, cv.hy);
+#pragma unroll
+                for (int l = 0; l < L; ++l) { a[l] = pq[phi_off[l]]; b[l] = rp0[l][0]; }
+                const V gz = grad<V, true>(LN::make(a), LN::make(b), cv.dz, cv.hz);
+                S* const dst = snode + ((z + 1) % NSLOT) * LY::NODE_SLOT;
+                node_store(dst, node_off, gx, gy, gz, rnT);
+                if (ring) {
+#pragma unroll
+                    for (int l = 0; l < L; ++l) { a[l] = pp[rphi_off[l] + 1]; b[l] = pp[rphi_off[l] - 1]; }
+                    const V rx = grad<V, true>(LN::make(a), LN::make(b), cv.dx, cv.hx);
+#pragma unroll
+                    for (int l = 0; l < L; ++l) { a[l] = pp[rphi_off[l] + TW]; b[l] = pp[rphi_off[l] - TW]; }
+                    const V ry = grad<V, true>(LN::make(a), LN::make(b), cv.dy, cv.hy);
+#pragma unroll
+                    for (int l = 0; l < L; ++l) { a[l] = pq[rphi_off[l]]; b[l] = p0[rphi_off[l]]; }
+                    const V rz = grad<V, true>(LN::make(a), LN::make(b), cv.dz, cv.hz);
+                    node_store(dst, rnode_off, rx, ry, rz, nullptr);
+                }
+            }
+            if (SOL && z + 1 <= nz - 1) {
+                S op[L];
+#pragma unroll
+                for (int l = 0; l < L; ++l) op[l] = rpp[l][0];
+                sol_plane(z + 1, pp, co[1], cr[0], rsT, op);
+            }
+        } else {
+            if (z + 1 >= 1 && z + 1 <= nz - 2) node_plane(z + 1, p0, pp, pq, nullptr);
+            if (SOL && z + 1 <= nz - 1) sol_plane(z + 1, pp, co[1], cr[0], nullptr, nullptr);
+        }
         // D: one barrier orders the plane; everyone learns of a failed load
         if (__syncthreads_or(bad)) {
             drain();
@@ -376,7 +471,7 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
         const S* const np1 = snode + ((z + 1) % NSLOT) * LY::NODE_SLOT;
         S PPs[L];
 #pragma unroll
-        for (int l = 0; l < L; ++l) PPs[l] = p0[phi_off[l]];
+        for (int l = 0; l < L; ++l) PPs[l] = ROLL ? rp0[l][0] : p0[phi_off[l]];
         const V PP = LN::make(PPs);
         const V CPP = LN::make(co[0]);
 
@@ -402,12 +497,22 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
 #define PF3D_NB(FIELD, PLANE, DELTA)                                         \
     _Pragma("unroll") for (int l = 0; l < L; ++l) t[l] = PLANE[phi_off[l] + (DELTA)]; \
     nb.FIELD = LN::make(t);
+#define PF3D_NR(FIELD, ARR, I)                                               \
+    _Pragma("unroll") for (int l = 0; l < L; ++l) t[l] = ARR[l][I];          \
+    nb.FIELD = LN::make(t);
             nb.PP = PP;
-            PF3D_NB(PN, p0, TW) PF3D_NB(PS, p0, -TW) PF3D_NB(PE, p0, 1) PF3D_NB(PW, p0, -1)
-            PF3D_NB(PT, pp, 0) PF3D_NB(PB, pm, 0)
+            if constexpr (ROLL) {
+                PF3D_NR(PN, rp0, 1) PF3D_NR(PS, rp0, 2) PF3D_NR(PE, rp0, 3) PF3D_NR(PW, rp0, 4)
+                PF3D_NR(PT, rpp, 0) PF3D_NR(PB, rpm, 0)
+                PF3D_NR(PNT, rpp, 1) PF3D_NR(PNB, rpm, 1) PF3D_NR(PST, rpp, 2) PF3D_NR(PSB, rpm, 2)
+                PF3D_NR(PET, rpp, 3) PF3D_NR(PEB, rpm, 3) PF3D_NR(PWT, rpp, 4) PF3D_NR(PWB, rpm, 4)
+            } else {
+                PF3D_NB(PN, p0, TW) PF3D_NB(PS, p0, -TW) PF3D_NB(PE, p0, 1) PF3D_NB(PW, p0, -1)
+                PF3D_NB(PT, pp, 0) PF3D_NB(PB, pm, 0)
+                PF3D_NB(PNT, pp, TW) PF3D_NB(PNB, pm, TW) PF3D_NB(PST, pp, -TW) PF3D_NB(PSB, pm, -TW)
+                PF3D_NB(PET, pp, 1) PF3D_NB(PEB, pm, 1) PF3D_NB(PWT, pp, -1) PF3D_NB(PWB, pm, -1)
+            }
             PF3D_NB(PNE, p0, TW + 1) PF3D_NB(PSE, p0, -TW + 1) PF3D_NB(PNW, p0, TW - 1) PF3D_NB(PSW, p0, -TW - 1)
-            PF3D_NB(PNT, pp, TW) PF3D_NB(PNB, pm, TW) PF3D_NB(PST, pp, -TW) PF3D_NB(PSB, pm, -TW)
-            PF3D_NB(PET, pp, 1) PF3D_NB(PEB, pm, 1) PF3D_NB(PWT, pp, -1) PF3D_NB(PWB, pm, -1)
 #undef PF3D_NB
             Node<V> E, W, N, So, Tt, B;
 #define PF3D_ND(NODE, Q, PLANE, DELTA, QI)                                   \
@@ -417,9 +522,19 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
             PF3D_ND(W, eps, n0, -1, 0) PF3D_ND(W, exy, n0, -1, 1) PF3D_ND(W, ezx, n0, -1, 3)
             PF3D_ND(N, eps, n0, NW, 0) PF3D_ND(N, exy, n0, NW, 1) PF3D_ND(N, eyz, n0, NW, 2)
             PF3D_ND(So, eps, n0, -NW, 0) PF3D_ND(So, exy, n0, -NW, 1) PF3D_ND(So, eyz, n0, -NW, 2)
-            PF3D_ND(Tt, eps, np1, 0, 0) PF3D_ND(Tt, eyz, np1, 0, 2) PF3D_ND(Tt, ezx, np1, 0, 3)
-            PF3D_ND(B, eps, nm1, 0, 0) PF3D_ND(B, eyz, nm1, 0, 2) PF3D_ND(B, ezx, nm1, 0, 3)
+            if constexpr (ROLL) {
+#define PF3D_NN(NODE, Q, ARR, I)                                             \
+    _Pragma("unroll") for (int l = 0; l < L; ++l) t[l] = ARR[l][I];          \
+    NODE.Q = LN::make(t);
+                PF3D_NN(Tt, eps, rnT, 0) PF3D_NN(Tt, eyz, rnT, 1) PF3D_NN(Tt, ezx, rnT, 2)
+                PF3D_NN(B, eps, rnB, 0) PF3D_NN(B, eyz, rnB, 1) PF3D_NN(B, ezx, rnB, 2)
+#undef PF3D_NN
+            } else {
+                PF3D_ND(Tt, eps, np1, 0, 0) PF3D_ND(Tt, eyz, np1, 0, 2) PF3D_ND(Tt, ezx, np1, 0, 3)
+                PF3D_ND(B, eps, nm1, 0, 0) PF3D_ND(B, eyz, nm1, 0, 2) PF3D_ND(B, ezx, nm1, 0, 3)
+            }
 #undef PF3D_ND
+#undef PF3D_NR
             E.eyz = W.eyz = N.ezx = So.ezx = Tt.exy = B.exy = V((S)0);   // unused by the body
             S rs[L];
 #pragma unroll
@@ -438,8 +553,17 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
                                                      b[l] = PLANE[node_off[l] + (DELTA) + NQ]; }  \
     q[I].br = LN::make(a);                                                                         \
     q[I].mu = LN::make(b);
-            PF3D_SN(0, s0, 0) PF3D_SN(1, s0, 1) PF3D_SN(2, s0, -1) PF3D_SN(3, s0, NW) PF3D_SN(4, s0, -NW)
-            PF3D_SN(5, sp1, 0) PF3D_SN(6, sm1, 0)
+            PF3D_SN(1, s0, 1) PF3D_SN(2, s0, -1) PF3D_SN(3, s0, NW) PF3D_SN(4, s0, -NW)
+            if constexpr (ROLL) {
+#define PF3D_SR(I, ARR)                                                                              \
+    _Pragma("unroll") for (int l = 0; l < L; ++l) { a[l] = ARR[l][0]; b[l] = ARR[l][1]; }           \
+    q[I].br = LN::make(a);                                                                           \
+    q[I].mu = LN::make(b);
+                PF3D_SR(0, rsP) PF3D_SR(5, rsT) PF3D_SR(6, rsB)
+#undef PF3D_SR
+            } else {
+                PF3D_SN(0, s0, 0) PF3D_SN(5, sp1, 0) PF3D_SN(6, sm1, 0)
+            }
 #undef PF3D_SN
             cn = conc_new<V, true>(PP, CPP, q[0], q[1], q[2], q[3], q[4], q[5], q[6], cv);
         }
@@ -513,26 +637,48 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
                 cr[0][l] = cr[1][l];
             }
         }
+        if constexpr (ROLL) {
+#pragma unroll
+            for (int l = 0; l < L; ++l) {
+#pragma unroll
+                for (int i = 0; i < 5; ++i) {
+                    rpm[l][i] = rp0[l][i];
+                    rp0[l][i] = rpp[l][i];
+                }
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    rnB[l][i] = rnC[l][i];
+                    rnC[l][i] = rnT[l][i];
+                }
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    rsB[l][i] = rsP[l][i];
+                    rsP[l][i] = rsT[l][i];
+                }
+            }
+        }
         s6 = (s6 + 1 == 6) ? 0 : s6 + 1;
-        if (NSLOT == 3) __syncthreads();   // the next plane's nodes overwrite plane z-1's slot
+        // window mode 3: the next plane's nodes overwrite plane z-1's slot
+        if constexpr (MarchWin<WIN>::two_barriers) __syncthreads();
     }
     return true;
 }
 
 // resident CTAs per SM the register budget is sized for (shared memory
-// allows no more): FP64 3, or 2 for a solute pass with 4-slot windows and for
-// a pass that may draw the smooth noise (its trilinear blend of eight hashes
-// needs about 128 registers); FP32 pairs 5 for a pass with the heat
-// equation, 4 otherwise; FP32 single cells 3
-template <typename S, int L, int NSLOT, bool SOL, bool HEAT, bool SMOOTH = false>
+// allows no more): FP64 3, or 2 -- 128 registers a thread -- for the rolled
+// window mode (its carried column values), a solute pass with 4-plane
+// windows and a pass that may draw the smooth noise (its trilinear blend of
+// eight hashes); FP32 pairs 5 for a pass with the heat equation, 4 otherwise
+// and in the rolled mode; FP32 single cells 3
+template <typename S, int L, int WIN, bool SOL, bool HEAT, bool SMOOTH = false>
 struct MarchOcc {
-    static constexpr int v = (sizeof(S) == 8) ? (((SOL && NSLOT == 4) || SMOOTH) ? 2 : 3)
-                                              : (L == 2 ? (HEAT ? 5 : 4) : 3);
+    static constexpr int v = (sizeof(S) == 8) ? ((WIN == 5 || (SOL && WIN == 4) || SMOOTH) ? 2 : 3)
+                                              : (L == 2 ? ((HEAT && WIN != 5) ? 5 : 4) : 3);
 };
 
 // single domain: one CTA per tile; the phase field comes through `tm`
-template <typename S, int L, int TY, int NSLOT, bool HEAT, bool DPPW, bool SOL, bool SMOOTH>
-__global__ void __launch_bounds__(32 * TY / L, (MarchOcc<S, L, NSLOT, SOL, HEAT, SMOOTH>::v))
+template <typename S, int L, int TY, int WIN, bool HEAT, bool DPPW, bool SOL, bool SMOOTH>
+__global__ void __launch_bounds__(32 * TY / L, (MarchOcc<S, L, WIN, SOL, HEAT, SMOOTH>::v))
     k_march(const __grid_constant__ CUtensorMap tm, DomainDesc d, const KC<S> c,
             const KC<typename Lanes<S, L>::V> cv, const S* __restrict__ c_in, S* __restrict__ phi_out,
             S* __restrict__ dpp, S* __restrict__ c_out, const S* __restrict__ T_old, S* __restrict__ T_new,
@@ -540,9 +686,9 @@ __global__ void __launch_bounds__(32 * TY / L, (MarchOcc<S, L, NSLOT, SOL, HEAT,
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char* smem = align128(smem_raw);
-    march_init_barriers<S, TY, SOL, NSLOT>(smem);
+    march_init_barriers<S, TY, SOL, MarchWin<WIN>::nslot>(smem);
     uint32_t par = 0;
-    if (!march_tile<S, L, TY, NSLOT, HEAT, DPPW, SOL, SMOOTH>(d, c, cv, &tm, c_in, phi_out, dpp, c_out, T_old,
+    if (!march_tile<S, L, TY, WIN, HEAT, DPPW, SOL, SMOOTH>(d, c, cv, &tm, c_in, phi_out, dpp, c_out, T_old,
                                                                 T_new, zchunk, blockIdx.x, blockIdx.y, blockIdx.z,
                                                                 smem, par)) {
         if (threadIdx.x == 0 && threadIdx.y == 0) atomicExch(err, kErrTmaTimeout);
@@ -553,9 +699,9 @@ __global__ void __launch_bounds__(32 * TY / L, (MarchOcc<S, L, NSLOT, SOL, HEAT,
 // pass of a step (temperatura + sweep 1, or the whole step with one sweep),
 // PASS 1 the last (sweep 2 + solute).  tmaps[2 d + b] describes buffer b of
 // domain d's phase field.
-template <typename S, int L, int TY, int NSLOT, int PASS, bool ONE_SWEEP, bool SMOOTH>
+template <typename S, int L, int TY, int WIN, int PASS, bool ONE_SWEEP, bool SMOOTH>
 __global__ void __launch_bounds__(32 * TY / L,
-                                  (MarchOcc<S, L, NSLOT, PASS == 1 || ONE_SWEEP, PASS == 0, SMOOTH>::v))
+                                  (MarchOcc<S, L, WIN, PASS == 1 || ONE_SWEEP, PASS == 0, SMOOTH>::v))
     k_march_batch(const BatchDomain* __restrict__ doms, const CUtensorMap* __restrict__ tmaps,
                   const BatchStep* __restrict__ steps, const BatchItem* __restrict__ items,
                   const int* __restrict__ n_items, int zchunk, int* __restrict__ err)
@@ -568,7 +714,7 @@ __global__ void __launch_bounds__(32 * TY / L,
     constexpr int nf = (int)(offsetof(KC<S>, hq) / sizeof(S));
     constexpr int NT = 32 * TY / L;
     unsigned char* smem = align128(smem_raw);
-    march_init_barriers<S, TY, SOL, NSLOT>(smem);
+    march_init_barriers<S, TY, SOL, MarchWin<WIN>::nslot>(smem);
     uint32_t par = 0;
     const int n = *n_items;
     const int tid = threadIdx.x + 32 * threadIdx.y;
@@ -599,16 +745,16 @@ __global__ void __launch_bounds__(32 * TY / L,
         if (PASS == 0) {
             const CUtensorMap* tm = tmaps + 2 * it.dom + q;
             if (ONE_SWEEP)
-                ok = march_tile<S, L, TY, NSLOT, true, true, true, SMOOTH>(
+                ok = march_tile<S, L, TY, WIN, true, true, true, SMOOTH>(
                     D.d, skc, kv, tm, (const S*)D.c[qc], (S*)D.phi[1 - q], (S*)D.dpp, (S*)D.c[1 - qc],
                     (const S*)D.T[qt], (S*)D.T[1 - qt], zchunk, it.bx, it.by, it.bz, smem, par);
             else
-                ok = march_tile<S, L, TY, NSLOT, true, false, false, SMOOTH>(
+                ok = march_tile<S, L, TY, WIN, true, false, false, SMOOTH>(
                     D.d, skc, kv, tm, (const S*)D.c[qc], (S*)D.phi[1 - q], (S*)D.dpp, nullptr, (const S*)D.T[qt],
                     (S*)D.T[1 - qt], zchunk, it.bx, it.by, it.bz, smem, par);
         } else {
             const CUtensorMap* tm = tmaps + 2 * it.dom + (1 - q);
-            ok = march_tile<S, L, TY, NSLOT, false, true, true, false>(
+            ok = march_tile<S, L, TY, WIN, false, true, true, false>(
                 D.d, skc, kv, tm, (const S*)D.c[qc], (S*)D.phi[q], (S*)D.dpp, (S*)D.c[1 - qc], nullptr, nullptr,
                 zchunk, it.bx, it.by, it.bz, smem, par);
         }
@@ -645,13 +791,13 @@ KC<typename Lanes<S, L>::V> kc_lanes(const KC<S>& k)
     }
 }
 
-template <typename S, int L, int TY, int NSLOT, bool HEAT, bool DPPW, bool SOL, bool SMOOTH>
+template <typename S, int L, int TY, int WIN, bool HEAT, bool DPPW, bool SOL, bool SMOOTH>
 cudaError_t launch_march_t(const CUtensorMap& tm, const DomainDesc& d, const StepArgs& s, const void* c_in,
                            void* phi_out, void* dpp, void* c_out, const void* T_old, void* T_new, int zchunk,
                            int* err, cudaStream_t st)
 {
-    using LY = MarchLayout<S, TY, SOL, NSLOT>;
-    auto kern = k_march<S, L, TY, NSLOT, HEAT, DPPW, SOL, SMOOTH>;
+    using LY = MarchLayout<S, TY, SOL, MarchWin<WIN>::nslot>;
+    auto kern = k_march<S, L, TY, WIN, HEAT, DPPW, SOL, SMOOTH>;
     static bool configured = false;   // one attribute call per instantiation
     if (!configured) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, LY::ALLOC);
@@ -669,51 +815,48 @@ cudaError_t launch_march_t(const CUtensorMap& tm, const DomainDesc& d, const Ste
 }
 
 // the passes of a step (32 x 8 tiles).  lanes: cells per thread (1 or 2);
-// nslot: node-window planes (3 or 4).  The smooth noise runs one cell per
-// thread.
+// win: window mode (3, 4 or 5, MarchWin).  The smooth noise runs one cell
+// per thread.
 template <typename S>
 cudaError_t launch_march_first(const CUtensorMap& tm, const DomainDesc& d, const StepArgs& s, const Fields& f,
-                               bool with_solute, int lanes, int nslot, int zchunk, int* err, cudaStream_t st)
+                               bool with_solute, int lanes, int win, int zchunk, int* err, cudaStream_t st)
 {
     const bool smooth = d.rt == 2;
 #define PF3D_MF(L, NS, DW, SO, SM)                                                                            \
     launch_march_t<S, L, 8, NS, true, DW, SO, SM>(tm, d, s, f.c_old, f.phi_mid, f.dpp, SO ? f.c_new : nullptr, \
                                                   f.T_old, f.T_new, zchunk, err, st)
-    if (smooth) {
-        if (with_solute) return nslot == 3 ? PF3D_MF(1, 3, true, true, true) : PF3D_MF(1, 4, true, true, true);
-        return nslot == 3 ? PF3D_MF(1, 3, false, false, true) : PF3D_MF(1, 4, false, false, true);
-    }
-    if (with_solute) {
-        if (lanes == 2) return nslot == 3 ? PF3D_MF(2, 3, true, true, false) : PF3D_MF(2, 4, true, true, false);
-        return nslot == 3 ? PF3D_MF(1, 3, true, true, false) : PF3D_MF(1, 4, true, true, false);
-    }
-    if (lanes == 2) return nslot == 3 ? PF3D_MF(2, 3, false, false, false) : PF3D_MF(2, 4, false, false, false);
-    return nslot == 3 ? PF3D_MF(1, 3, false, false, false) : PF3D_MF(1, 4, false, false, false);
+#define PF3D_MW(L, DW, SO, SM) \
+    (win == 3 ? PF3D_MF(L, 3, DW, SO, SM) : win == 4 ? PF3D_MF(L, 4, DW, SO, SM) : PF3D_MF(L, 5, DW, SO, SM))
+    if (smooth) return with_solute ? PF3D_MW(1, true, true, true) : PF3D_MW(1, false, false, true);
+    if (with_solute) return lanes == 2 ? PF3D_MW(2, true, true, false) : PF3D_MW(1, true, true, false);
+    return lanes == 2 ? PF3D_MW(2, false, false, false) : PF3D_MW(1, false, false, false);
+#undef PF3D_MW
 #undef PF3D_MF
 }
 
 template <typename S>
 cudaError_t launch_march_last(const CUtensorMap& tm, const DomainDesc& d, const StepArgs& s, const Fields& f,
-                              int lanes, int nslot, int zchunk, int* err, cudaStream_t st)
+                              int lanes, int win, int zchunk, int* err, cudaStream_t st)
 {
 #define PF3D_ML(L, NS)                                                                                     \
     launch_march_t<S, L, 8, NS, false, true, true, false>(tm, d, s, f.c_old, f.phi_new, f.dpp, f.c_new, nullptr, \
                                                           nullptr, zchunk, err, st)
-    if (lanes == 2) return nslot == 3 ? PF3D_ML(2, 3) : PF3D_ML(2, 4);
-    return nslot == 3 ? PF3D_ML(1, 3) : PF3D_ML(1, 4);
+#define PF3D_MW(L) (win == 3 ? PF3D_ML(L, 3) : win == 4 ? PF3D_ML(L, 4) : PF3D_ML(L, 5))
+    return lanes == 2 ? PF3D_MW(2) : PF3D_MW(1);
+#undef PF3D_MW
 #undef PF3D_ML
 }
 
 // The persistent grid is the SM count times the CTAs of this kernel that are
 // resident on one SM.
-template <typename S, int L, int NSLOT, int PASS, bool ONE_SWEEP, bool SMOOTH>
+template <typename S, int L, int WIN, int PASS, bool ONE_SWEEP, bool SMOOTH>
 cudaError_t launch_march_batch_t(const BatchDomain* doms, const CUtensorMap* tmaps, const BatchStep* steps,
                                  const BatchItem* items, const int* n_items, int zchunk, int n_sm, int* err,
                                  cudaStream_t st)
 {
     constexpr bool SOL = PASS == 1 || ONE_SWEEP;
-    using LY = MarchLayout<S, 8, SOL, NSLOT>;
-    auto kern = k_march_batch<S, L, 8, NSLOT, PASS, ONE_SWEEP, SMOOTH>;
+    using LY = MarchLayout<S, 8, SOL, MarchWin<WIN>::nslot>;
+    auto kern = k_march_batch<S, L, 8, WIN, PASS, ONE_SWEEP, SMOOTH>;
     static int per_sm = 0;   // one attribute and occupancy query per instantiation
     if (per_sm == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, LY::ALLOC);
@@ -730,24 +873,19 @@ cudaError_t launch_march_batch_t(const BatchDomain* doms, const CUtensorMap* tma
 template <typename S>
 cudaError_t launch_march_batch(const BatchDomain* doms, const CUtensorMap* tmaps, const BatchStep* steps,
                                const BatchItem* items, const int* n_items, int pass, bool one_sweep, bool smooth,
-                               int lanes, int nslot, int zchunk, int n_sm, int* err, cudaStream_t st)
+                               int lanes, int win, int zchunk, int n_sm, int* err, cudaStream_t st)
 {
 #define PF3D_MB(L, NS, P, ONE, SM) \
     launch_march_batch_t<S, L, NS, P, ONE, SM>(doms, tmaps, steps, items, n_items, zchunk, n_sm, err, st)
+#define PF3D_MW(L, P, ONE, SM) \
+    (win == 3 ? PF3D_MB(L, 3, P, ONE, SM) : win == 4 ? PF3D_MB(L, 4, P, ONE, SM) : PF3D_MB(L, 5, P, ONE, SM))
     if (pass == 0) {
-        if (smooth) {
-            if (one_sweep) return nslot == 3 ? PF3D_MB(1, 3, 0, true, true) : PF3D_MB(1, 4, 0, true, true);
-            return nslot == 3 ? PF3D_MB(1, 3, 0, false, true) : PF3D_MB(1, 4, 0, false, true);
-        }
-        if (lanes == 2) {
-            if (one_sweep) return nslot == 3 ? PF3D_MB(2, 3, 0, true, false) : PF3D_MB(2, 4, 0, true, false);
-            return nslot == 3 ? PF3D_MB(2, 3, 0, false, false) : PF3D_MB(2, 4, 0, false, false);
-        }
-        if (one_sweep) return nslot == 3 ? PF3D_MB(1, 3, 0, true, false) : PF3D_MB(1, 4, 0, true, false);
-        return nslot == 3 ? PF3D_MB(1, 3, 0, false, false) : PF3D_MB(1, 4, 0, false, false);
+        if (smooth) return one_sweep ? PF3D_MW(1, 0, true, true) : PF3D_MW(1, 0, false, true);
+        if (lanes == 2) return one_sweep ? PF3D_MW(2, 0, true, false) : PF3D_MW(2, 0, false, false);
+        return one_sweep ? PF3D_MW(1, 0, true, false) : PF3D_MW(1, 0, false, false);
     }
-    if (lanes == 2) return nslot == 3 ? PF3D_MB(2, 3, 1, false, false) : PF3D_MB(2, 4, 1, false, false);
-    return nslot == 3 ? PF3D_MB(1, 3, 1, false, false) : PF3D_MB(1, 4, 1, false, false);
+    return lanes == 2 ? PF3D_MW(2, 1, false, false) : PF3D_MW(1, 1, false, false);
+#undef PF3D_MW
 #undef PF3D_MB
 }
 

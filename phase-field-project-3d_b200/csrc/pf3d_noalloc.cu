@@ -63,6 +63,11 @@ struct NSum {
     }
 };
 
+// max / min that return NaN when either argument is NaN, as pf_diagnosticos
+// reports them (fmax/fmin would drop a NaN and show finite extremes)
+__device__ __forceinline__ double nan_max(double a, double b) { return (a > b || a != a) ? a : b; }
+__device__ __forceinline__ double nan_min(double a, double b) { return (a < b || a != a) ? a : b; }
+
 struct PlaneArgs {
     int nx, ny, nz;
     int runs;              // S: runs of cells per plane, one CTA and one row each
@@ -89,8 +94,8 @@ __global__ void __launch_bounds__(256) k_diag_plane(PlaneArgs a, const T* __rest
         const long long id = (long long)x + (long long)y * a.px + (long long)z * a.plane;
         const double p = (double)phi[id];
         l2.add(__dmul_rn(p, p));
-        mx = fmax(mx, p);
-        mn = fmin(mn, p);
+        mx = nan_max(mx, p);
+        mn = nan_min(mn, p);
         sol.add((double)c[id]);
         const double w = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(a.W0, p), p), __dsub_rn(1.0, p)), __dsub_rn(1.0, p));
         double g2 = 0.0;
@@ -109,7 +114,7 @@ __global__ void __launch_bounds__(256) k_diag_plane(PlaneArgs a, const T* __rest
         double o[kRow];
         for (int k = 0; k < kRow; ++k) o[k] = __shfl_down_sync(0xffffffffu, v[k], off);
         NSum s1{v[0], v[1]}; s1.merge(o[0], o[1]); v[0] = s1.s; v[1] = s1.c;
-        v[2] = fmax(v[2], o[2]); v[3] = fmin(v[3], o[3]);
+        v[2] = nan_max(v[2], o[2]); v[3] = nan_min(v[3], o[3]);
         NSum s2{v[4], v[5]}; s2.merge(o[4], o[5]); v[4] = s2.s; v[5] = s2.c;
         NSum s3{v[6], v[7]}; s3.merge(o[6], o[7]); v[6] = s3.s; v[7] = s3.c;
     }
@@ -121,7 +126,7 @@ __global__ void __launch_bounds__(256) k_diag_plane(PlaneArgs a, const T* __rest
         for (int k = 0; k < kRow; ++k) v[k] = sh[0][k];
         for (int ww = 1; ww < (int)(blockDim.x >> 5); ++ww) {
             NSum s1{v[0], v[1]}; s1.merge(sh[ww][0], sh[ww][1]); v[0] = s1.s; v[1] = s1.c;
-            v[2] = fmax(v[2], sh[ww][2]); v[3] = fmin(v[3], sh[ww][3]);
+            v[2] = nan_max(v[2], sh[ww][2]); v[3] = nan_min(v[3], sh[ww][3]);
             NSum s2{v[4], v[5]}; s2.merge(sh[ww][4], sh[ww][5]); v[4] = s2.s; v[5] = s2.c;
             NSum s3{v[6], v[7]}; s3.merge(sh[ww][6], sh[ww][7]); v[6] = s3.s; v[7] = s3.c;
         }
@@ -137,8 +142,8 @@ __global__ void k_diag_plane_final(const double* __restrict__ part, int rows, do
     for (int r = 0; r < rows; ++r) {
         const double* p = part + (long long)r * kRow;
         l2.merge(p[0], p[1]);
-        mx = fmax(mx, p[2]);
-        mn = fmin(mn, p[3]);
+        mx = nan_max(mx, p[2]);
+        mn = nan_min(mn, p[3]);
         sol.merge(p[4], p[5]);
         fe.merge(p[6], p[7]);
     }

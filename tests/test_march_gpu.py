@@ -8,7 +8,8 @@ every field after N steps must carry the bits of the cp.async passes: on
 grids down to the 5-cell minimum, ragged tile edges, tiles that are all
 boundary, z-chunks that split the domain anywhere, one, two and three
 sweeps, every noise kind, quintic h, heat diffusion, one and two cells per
-thread, both window sizes, both precisions."""
+thread, every window mode (3- and 4-plane windows, the own column rolled in
+registers), both precisions."""
 import numpy as np
 import pytest
 
@@ -56,7 +57,7 @@ SHAPES = [
 def test_march_equals_cpasync_passes(gpu, prec, shape, over):
     g, p, st = case(*shape, **over)
     want, sw = run(g, p, st, prec, 5, kernel=0, paired=0)
-    for paired, nslot, zchunk in ((0, 3, 64), (2, 4, 64), (2, 3, 7), (0, 4, 4)):
+    for paired, nslot, zchunk in ((0, 3, 64), (2, 4, 64), (2, 3, 7), (0, 4, 4), (0, 5, 64), (2, 5, 5)):
         got, sg = run(g, p, st, prec, 5, kernel=1, paired=paired, nslot=nslot, zchunk=zchunk)
         for k in want:
             assert np.array_equal(got[k], want[k]), (k, paired, nslot, zchunk)
@@ -78,7 +79,7 @@ def test_march_status_word_clean_after_steps(gpu):
 def test_march_batch_equals_cpasync_batch(gpu, prec, sweeps):
     """A batch of uneven small domains (tiles that are all boundary, ragged
     edges, mixed noise kinds) on the TMA passes, with one and two cells per
-    thread and both window sizes, against the same batch on the cp.async
+    thread and every window mode, against the same batch on the cp.async
     passes; a domain leaves mid-run at its target step."""
     cases = [case(40, 33, 50, n_varreduras=sweeps), case(21, 64, 17, T0=918.0, taxa_resfr=30.0, n_varreduras=sweeps),
              case(70, 12, 35, AAA=0.02, ruido_tipo=1, n_varreduras=sweeps),
@@ -102,7 +103,7 @@ def test_march_batch_equals_cpasync_batch(gpu, prec, sweeps):
             return [b.fields(s) for s in slots], [b.state(s).it for s in slots]
 
     want, wit = run(0, 0, 0)
-    for paired, nslot in ((0, 3), (1, 4), (1, 3)):
+    for paired, nslot in ((0, 3), (1, 4), (1, 3), (0, 5), (1, 5)):
         got, git = run(1, paired, nslot)
         assert git == wit
         for i, (a, b) in enumerate(zip(got, want)):
