@@ -106,9 +106,22 @@ __device__ __forceinline__ S heat_at(const S* __restrict__ T_old, long long id, 
     return heat_new<S>(PP, dppv, TE, TW, TN, TS, TT, TB, c);
 }
 
+// (a + k) mod N for a in [0, N) and k in [0, N)
+template <int N>
+__device__ __forceinline__ int wrap_add(int a, int k)
+{
+    const int t = a + k;
+    return t >= N ? t - N : t;
+}
+
+// the dynamic shared-memory base rounded up to 128 bytes.  The offset is
+// added to the shared array itself (not computed through an integer cast of
+// its address), so the compiler still knows every pointer derived from it
+// is a shared-memory pointer and emits shared loads and stores, not generic
+// ones with 64-bit address arithmetic.
 __device__ __forceinline__ unsigned char* align128(unsigned char* p)
 {
-    return reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(p) + 127) & ~uintptr_t(127));
+    return p + ((128u - (smem_u32(p) & 127u)) & 127u);
 }
 
 // Initialises the six plane barriers of a tile's window (one thread), made
@@ -205,15 +218,13 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
 
     // ---- plane loads ----
     uint32_t pend = 0;          // slots with a load issued and not yet seen complete (lead thread)
-    auto issue = [&](int p) {   // one thread: plane p into its slot
-        const int s = (p + 6) % 6;
+    auto issue = [&](int p, int s) {   // one thread: plane p into its slot s = p mod 6
         const uint32_t bar = bar0 + 8 * s;
         mbar_arrive_expect_tx(bar, (uint32_t)LY::PHI_BYTES);
         tma_load_3d(smem_u32(sphi + s * LY::PHI_SLOT), tm, x0 - XOFF, y0 - 2, p, bar);
         pend |= 1u << s;
     };
-    auto wait_plane = [&](int p) -> bool {
-        const int s = (p + 6) % 6;
+    auto wait_plane = [&](int s) -> bool {   // the load into slot s has landed
         const bool ok = mbar_wait(bar0 + 8 * s, (par >> s) & 1u);
         if (ok) {
             par ^= 1u << s;
@@ -251,8 +262,8 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
     };
     // node quantities of plane n into its slot, from phase planes n-1, n, n+1
     // in shared memory (own items' values also into `keep` when given)
-    auto node_plane = [&](int n, const S* pm, const S* p0, const S* pp, S (*keep)[3]) {
-        S* dst = snode + ((n + NSLOT) % NSLOT) * LY::NODE_SLOT;
+    auto node_plane = [&](int sl, const S* pm, const S* p0, const S* pp, S (*keep)[3]) {
+        S* dst = snode + sl * LY::NODE_SLOT;
         auto one = [&](const int* off_phi, const int* off_node, S (*kp)[3]) {
             S a[L], b[L];
 #pragma unroll
@@ -273,8 +284,8 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
     // and the concentration of that plane at the own (co) and ring (cr)
     // points; the own points' values also into `keep` when given, and their
     // phase values taken from `ownp` when given
-    auto sol_plane = [&](int s, const S* p0, const S* co, const S* cr, S (*keep)[2], const S* ownp) {
-        S* dst = ssol + ((s + NSLOT) % NSLOT) * LY::SOL_SLOT;
+    auto sol_plane = [&](int sl, const S* p0, const S* co, const S* cr, S (*keep)[2], const S* ownp) {
+        S* dst = ssol + sl * LY::SOL_SLOT;
         auto one = [&](const int* off_phi, const int* off_node, const S* cc, S (*kp)[2], const S* op) {
             S a[L];
 #pragma unroll
@@ -329,7 +340,7 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
     if (lead) {
         fence_proxy_async_smem();   // the slots may hold a previous tile's planes
         for (int p = zb - 2; p <= zb + 3; ++p)
-            if (p >= 0 && p <= zlast) issue(p);
+            if (p >= 0 && p <= zlast) issue(p, (p + 6) % 6);
     }
     S co[3][L], cr[2][L];   // concentration: own points of planes z, z+1, z+2; ring points of z+1, z+2
     S nd[L], nt[L];         // centre values of the next plane: DPP (or the noise), TOLD
@@ -373,22 +384,25 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
         load_c(zb, co[0], cr[0]);
         load_c(zb + 1, co[1], cr[1]);
         for (int p = zb - 2; p <= zb + 1; ++p)
-            if (p >= 0 && p <= zlast) bad |= !wait_plane(p);
-        if (zb - 1 >= 0) sol_plane(zb - 1, sphi + ((zb + 5) % 6) * LY::PHI_SLOT, ca, cra, ROLL ? rsB : nullptr, nullptr);
-        sol_plane(zb, sphi + (zb % 6) * LY::PHI_SLOT, co[0], cr[0], ROLL ? rsP : nullptr, nullptr);
+            if (p >= 0 && p <= zlast) bad |= !wait_plane((p + 6) % 6);
+        if (zb - 1 >= 0)
+            sol_plane(wrap_add<NSLOT>(zb % NSLOT, NSLOT - 1), sphi + ((zb + 5) % 6) * LY::PHI_SLOT, ca, cra,
+                      ROLL ? rsB : nullptr, nullptr);
+        sol_plane(zb % NSLOT, sphi + (zb % 6) * LY::PHI_SLOT, co[0], cr[0], ROLL ? rsP : nullptr, nullptr);
 #pragma unroll
         for (int l = 0; l < L; ++l) cr[0][l] = cr[1][l];
     } else {
         load_c(zb, co[0], cr[0]);
         for (int p = zb - 2; p <= zb + 1; ++p)
-            if (p >= 0 && p <= zlast) bad |= !wait_plane(p);
+            if (p >= 0 && p <= zlast) bad |= !wait_plane((p + 6) % 6);
     }
     load_centre(zb);
     if (zb - 1 >= 1 && zb - 1 <= nz - 2)
-        node_plane(zb - 1, sphi + ((zb + 4) % 6) * LY::PHI_SLOT, sphi + ((zb + 5) % 6) * LY::PHI_SLOT,
+        node_plane(wrap_add<NSLOT>(zb % NSLOT, NSLOT - 1), sphi + ((zb + 4) % 6) * LY::PHI_SLOT,
+                   sphi + ((zb + 5) % 6) * LY::PHI_SLOT,
                    sphi + (zb % 6) * LY::PHI_SLOT, ROLL ? rnB : nullptr);
     if (zb >= 1 && zb <= nz - 2)
-        node_plane(zb, sphi + ((zb + 5) % 6) * LY::PHI_SLOT, sphi + (zb % 6) * LY::PHI_SLOT,
+        node_plane(zb % NSLOT, sphi + ((zb + 5) % 6) * LY::PHI_SLOT, sphi + (zb % 6) * LY::PHI_SLOT,
                    sphi + ((zb + 1) % 6) * LY::PHI_SLOT, ROLL ? rnC : nullptr);
     load5(rpm, sphi + ((zb + 5) % 6) * LY::PHI_SLOT);
     load5(rp0, sphi + (zb % 6) * LY::PHI_SLOT);
@@ -397,13 +411,16 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
     uint64_t hin[L];   // noise hash input of the own cells, carried along z (k = z + 1)
 #pragma unroll
     for (int l = 0; l < L; ++l) hin[l] = hash_base(x + 1, yv[l] + 1, c.it, 1) + (uint64_t)(zb + 1) * kHashK;
-    int s6 = zb % 6;   // phase slot of plane z
+    int s6 = zb % 6;       // phase slot of plane z
+    int sn = zb % NSLOT;   // node / point slot of plane z
 
     for (int z = zb; z < ze; ++z, zoff += pl) {
-        const S* const pm = sphi + ((s6 + 5) % 6) * LY::PHI_SLOT;
+        const int s6p1 = wrap_add<6>(s6, 1), s6p2 = wrap_add<6>(s6, 2);
+        const int snm1 = wrap_add<NSLOT>(sn, NSLOT - 1), snp1 = wrap_add<NSLOT>(sn, 1);
+        const S* const pm = sphi + wrap_add<6>(s6, 5) * LY::PHI_SLOT;
         const S* const p0 = sphi + s6 * LY::PHI_SLOT;
-        const S* const pp = sphi + ((s6 + 1) % 6) * LY::PHI_SLOT;
-        const S* const pq = sphi + ((s6 + 2) % 6) * LY::PHI_SLOT;
+        const S* const pp = sphi + s6p1 * LY::PHI_SLOT;
+        const S* const pq = sphi + s6p2 * LY::PHI_SLOT;
         S dcur[L], tcur[L];
 #pragma unroll
         for (int l = 0; l < L; ++l) { dcur[l] = nd[l]; tcur[l] = nt[l]; }
@@ -412,7 +429,7 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
         else load_c(z + 1, co[1], cr[1]);
 
         // A: plane z+2 has landed
-        if (z + 2 <= zlast) bad |= !wait_plane(z + 2);
+        if (z + 2 <= zlast) bad |= !wait_plane(s6p2);
         // B, C: nodes and solute points of plane z+1
         if constexpr (ROLL) {
             load5(rpp, pp);   // plane z+1 at the own column: the stencil's T values and the node's x/y gradient
@@ -427,7 +444,7 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
 #pragma unroll
                 for (int l = 0; l < L; ++l) { a[l] = pq[phi_off[l]]; b[l] = rp0[l][0]; }
                 const V gz = grad<V, true>(LN::make(a), LN::make(b), cv.dz, cv.hz);
-                S* const dst = snode + ((z + 1) % NSLOT) * LY::NODE_SLOT;
+                S* const dst = snode + snp1 * LY::NODE_SLOT;
                 node_store(dst, node_off, gx, gy, gz, rnT);
                 if (ring) {
 #pragma unroll
@@ -446,11 +463,11 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
                 S op[L];
 #pragma unroll
                 for (int l = 0; l < L; ++l) op[l] = rpp[l][0];
-                sol_plane(z + 1, pp, co[1], cr[0], rsT, op);
+                sol_plane(snp1, pp, co[1], cr[0], rsT, op);
             }
         } else {
-            if (z + 1 >= 1 && z + 1 <= nz - 2) node_plane(z + 1, p0, pp, pq, nullptr);
-            if (SOL && z + 1 <= nz - 1) sol_plane(z + 1, pp, co[1], cr[0], nullptr, nullptr);
+            if (z + 1 >= 1 && z + 1 <= nz - 2) node_plane(snp1, p0, pp, pq, nullptr);
+            if (SOL && z + 1 <= nz - 1) sol_plane(snp1, pp, co[1], cr[0], nullptr, nullptr);
         }
         // D: one barrier orders the plane; everyone learns of a failed load
         if (__syncthreads_or(bad)) {
@@ -460,15 +477,15 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
         // E: the load of plane z+4 into the slot plane z-2 has left
         if (lead && z + 4 <= zlast) {
             fence_proxy_async_smem();
-            issue(z + 4);
+            issue(z + 4, wrap_add<6>(s6, 4));
         }
 
         // F: the cells of plane z
         const bool zin = z >= 1 && z <= nz - 2;   // T interior / phase source / solute interior
         const bool zph = z >= 2 && z <= nz - 3;   // phase interior
-        const S* const nm1 = snode + ((z - 1 + NSLOT) % NSLOT) * LY::NODE_SLOT;
-        const S* const n0 = snode + (z % NSLOT) * LY::NODE_SLOT;
-        const S* const np1 = snode + ((z + 1) % NSLOT) * LY::NODE_SLOT;
+        const S* const nm1 = snode + snm1 * LY::NODE_SLOT;
+        const S* const n0 = snode + sn * LY::NODE_SLOT;
+        const S* const np1 = snode + snp1 * LY::NODE_SLOT;
         S PPs[L];
 #pragma unroll
         for (int l = 0; l < L; ++l) PPs[l] = ROLL ? rp0[l][0] : p0[phi_off[l]];
@@ -543,9 +560,9 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
         }
         V cn = CPP;
         if (SOL && zin) {
-            const S* const sm1 = ssol + ((z - 1 + NSLOT) % NSLOT) * LY::SOL_SLOT;
-            const S* const s0 = ssol + (z % NSLOT) * LY::SOL_SLOT;
-            const S* const sp1 = ssol + ((z + 1) % NSLOT) * LY::SOL_SLOT;
+            const S* const sm1 = ssol + snm1 * LY::SOL_SLOT;
+            const S* const s0 = ssol + sn * LY::SOL_SLOT;
+            const S* const sp1 = ssol + snp1 * LY::SOL_SLOT;
             SolNode<V> q[7];   // P, E, W, N, S, T, B
             S a[L], b[L];
 #define PF3D_SN(I, PLANE, DELTA)                                                                   \
@@ -657,7 +674,8 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
                 }
             }
         }
-        s6 = (s6 + 1 == 6) ? 0 : s6 + 1;
+        s6 = s6p1;
+        sn = snp1;
         // window mode 3: the next plane's nodes overwrite plane z-1's slot
         if constexpr (MarchWin<WIN>::two_barriers) __syncthreads();
     }
