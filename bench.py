@@ -60,17 +60,23 @@ def step_hbm_frac_of(gbs: float, peak: float) -> float:
     return gbs / peak
 
 
-def ncu_traffic(kernel: str, precision: int):
-    """Per-cell DRAM bytes of a fused pass from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+def ncu_figures(kernel: str, precision: int) -> dict:
+    """Per-cell figures of a fused pass from the committed ncu summary
+    (profiles/ncu_passes.txt: `<pass> fp<NN> key=value ...`): DRAM bytes,
+    executed thread instructions and FP64 flops per cell, issue-active and
+    FP64-pipe fractions of the captured launch."""
+    path = os.path.join(ROOT, "profiles", "ncu_passes.txt")
+    out = {}
     try:
         for line in open(path):
             t = line.split()
-            if len(t) >= 3 and t[0] == kernel and t[1] == f"fp{precision}":
-                return float(t[2].split("=")[1])
+            if len(t) >= 3 and not t[0].startswith("#") and t[0] == kernel and t[1] == f"fp{precision}":
+                for kv in t[2:]:
+                    k, v = kv.split("=")
+                    out[k] = float(v)
     except Exception:
         pass
-    return None
+    return out
 
 
 class ClockSampler:
@@ -378,8 +384,31 @@ def main():
     alg_bytes = PASS_BYTES_PER_CELL[kname][prec] * cells
     avg_s = ms_k / max(1, n_k) / 1e3
     achieved = alg_bytes / avg_s / 1e9
-    tr = ncu_traffic(kname, prec)
+    fig = ncu_figures(kname, prec)
+    tr = fig.get("dram_bytes_per_cell")
     step_gbs = value / world * STEP_BYTES_PER_CELL[prec]
+    # the other two ceilings of the dominant pass, from this run's kernel time
+    # and the per-cell counts of its ncu capture: the FP64 pipe (nominal peak
+    # 148 SMs x 64 FP64 FMA a clock x 2 flops at the sampled SM clock) and
+    # instruction issue (148 SMs x 4 schedulers x 1 warp instruction a clock)
+    clk_hz = (clk["sm_mhz"] if clk and clk.get("sm_mhz") else 1965.0) * 1e6
+    n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+    ceilings = {"hbm": (tr * cells / avg_s / 1e9) / peak if tr else achieved / peak}
+    fp64 = None
+    if prec == 64 and "fp64_flops_per_cell" in fig:
+        peak_tf = n_sm * 64 * 2 * clk_hz / 1e12
+        tf = fig["fp64_flops_per_cell"] * cells / avg_s / 1e12
+        other = ncu_figures("fused_first" if kname == "fused_last" else "fused_last", prec)
+        step_flops = fig["fp64_flops_per_cell"] + other.get("fp64_flops_per_cell", 0.0)
+        step_tf = step_flops * cells * args.steps * world / (ms / 1e3) / 1e12 / world
+        fp64 = {"achieved_tflops": tf, "peak_tflops": peak_tf, "frac": tf / peak_tf,
+                "flops_per_cell": fig["fp64_flops_per_cell"],
+                "step": {"flops_per_cell": step_flops, "achieved_tflops": step_tf, "frac": step_tf / peak_tf},
+                "peak_source": f"nominal: {n_sm} SMs x 64 FP64 FMA/clock x 2 at the sampled {clk_hz / 1e6:.0f} MHz"}
+        ceilings["fp64_pipe"] = tf / peak_tf
+    if "inst_per_cell" in fig:
+        ceilings["issue"] = fig["inst_per_cell"] / 32 * cells / avg_s / (n_sm * 4 * clk_hz)
+    limiter = max(ceilings, key=ceilings.get)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": (tr * cells if tr is not None else None), "kernel": kname,
                 "kernel_ms": avg_s * 1e3, "peak_source": f"{peak_kind} hbm_gbs",
@@ -387,7 +416,10 @@ def main():
                 "shares": {"fused_first": mf / max(1e-9, mf + ml), "fused_last": ml / max(1e-9, mf + ml)},
                 "step": {"achieved": step_gbs, "frac": step_hbm_frac_of(step_gbs, peak),
                          "alg_bytes_per_cell": STEP_BYTES_PER_CELL[prec]},
-                "limiter": "instruction issue, not HBM (ncu: 69-78 % issue active, DRAM 8-22 % of peak)"}
+                "fp64": fp64,
+                "ceiling_fracs": ceilings,
+                "limiter": limiter,
+                "ncu_figures": fig}
     step_hbm_frac = step_gbs / peak
 
     # ---- end to end through the C-ABI with pinned host buffers ----
