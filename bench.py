@@ -395,17 +395,23 @@ def main():
     n_sm = torch.cuda.get_device_properties(local).multi_processor_count
     ceilings = {"hbm": (tr * cells / avg_s / 1e9) / peak if tr else achieved / peak}
     fp64 = None
-    if prec == 64 and "fp64_flops_per_cell" in fig:
-        peak_tf = n_sm * 64 * 2 * clk_hz / 1e12
-        tf = fig["fp64_flops_per_cell"] * cells / avg_s / 1e12
+    if prec == 64 and "fp64_inst_per_cell" in fig:
+        # FP64 pipe: lane-operations (DFMA, DMUL, DADD) per second against
+        # 64 a clock per SM; flops count an FMA as two
+        peak_ops = n_sm * 64 * clk_hz
+        ops = fig["fp64_inst_per_cell"] * cells / avg_s
         other = ncu_figures("fused_first" if kname == "fused_last" else "fused_last", prec)
-        step_flops = fig["fp64_flops_per_cell"] + other.get("fp64_flops_per_cell", 0.0)
-        step_tf = step_flops * cells * args.steps * world / (ms / 1e3) / 1e12 / world
-        fp64 = {"achieved_tflops": tf, "peak_tflops": peak_tf, "frac": tf / peak_tf,
-                "flops_per_cell": fig["fp64_flops_per_cell"],
-                "step": {"flops_per_cell": step_flops, "achieved_tflops": step_tf, "frac": step_tf / peak_tf},
-                "peak_source": f"nominal: {n_sm} SMs x 64 FP64 FMA/clock x 2 at the sampled {clk_hz / 1e6:.0f} MHz"}
-        ceilings["fp64_pipe"] = tf / peak_tf
+        step_ops = (fig["fp64_inst_per_cell"] + other.get("fp64_inst_per_cell", 0.0)) * cells * args.steps / (ms / 1e3)
+        step_flops = fig.get("fp64_flops_per_cell", 0.0) + other.get("fp64_flops_per_cell", 0.0)
+        fp64 = {"achieved_tflops": fig.get("fp64_flops_per_cell", 0.0) * cells / avg_s / 1e12,
+                "peak_tflops": 2 * peak_ops / 1e12, "pipe_frac": ops / peak_ops,
+                "inst_per_cell": fig["fp64_inst_per_cell"], "flops_per_cell": fig.get("fp64_flops_per_cell"),
+                "step": {"inst_per_cell": fig["fp64_inst_per_cell"] + other.get("fp64_inst_per_cell", 0.0),
+                         "flops_per_cell": step_flops, "pipe_frac": step_ops / peak_ops,
+                         "achieved_tflops": step_flops * cells * args.steps / (ms / 1e3) / 1e12},
+                "peak_source": f"nominal: {n_sm} SMs x 64 FP64 lane-operations a clock at the sampled "
+                               f"{clk_hz / 1e6:.0f} MHz"}
+        ceilings["fp64_pipe"] = ops / peak_ops
     if "inst_per_cell" in fig:
         ceilings["issue"] = fig["inst_per_cell"] / 32 * cells / avg_s / (n_sm * 4 * clk_hz)
     limiter = max(ceilings, key=ceilings.get)
