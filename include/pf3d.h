@@ -37,9 +37,9 @@ extern "C" {
 #define PF_E_NOMEM (-3)    /* device allocation refused or over budget      */
 #define PF_E_STATE (-4)    /* call not valid in the current state           */
 #define PF_E_NODEV (-5)    /* no CUDA device visible                        */
-#define PF_E_NONFINITE (-7) /* the diagnostics found cells whose phi or c is
-                              not finite (the run has blown up); the five
-                              values are still returned, max/min as NaN   */
+#define PF_E_NONFINITE (-7) /* the diagnostics found cells whose phi, c, T
+                              or DPP is not finite (the run has blown up);
+                              the five values are still returned          */
 #define PF_E_KERNEL (-6)   /* a kernel reported a failure in the context's
                               status word (a TMA plane load that did not
                               arrive within its bounded wait); reported by
@@ -198,8 +198,10 @@ int pf_concentracao_soluto(pf_ctx* ctx);
 int pf_auxiliar(const pf_ctx* ctx, double TP, double Cs_eq, double Cl_eq, double* M0);
 /* diagnosticos.f90: out = {L2_phi, phi_max, phi_min, solute_total,
    free_energy} of phase_field_new / conc_soluto_new.  Watchdog: the same
-   reduction counts the cells whose phi or c is not finite; if any, max/min
-   come back NaN and the call returns PF_E_NONFINITE (out still filled).    */
+   reduction counts the cells where phi, c, TNEW or DPP is not finite (the
+   clamp of the phase update turns a NaN update into 1, so a blow-up can
+   show only in DPP and T); if any, the call returns PF_E_NONFINITE with out
+   still filled (max/min NaN when phi holds the NaN).                       */
 int pf_diagnosticos(pf_ctx* ctx, double out[5]);
 /* principal.f90:200-226: old <- new for phi, T and c.  Done by exchanging
    buffers: afterwards the "new" arrays hold the previous "old" data until

@@ -462,10 +462,11 @@ int pf_auxiliar(const pf_ctx* ctx, double TP, double Cs_eq, double Cl_eq, double
     return pf_auxiliar_scalar(&ctx->p, ctx->dv.E0, ctx->dv.W0, TP, Cs_eq, Cl_eq, M0);
 }
 
-static int run_diag(pf_ctx* ctx, const void* phi, const void* c, double out[5])
+static int run_diag(pf_ctx* ctx, const void* phi, const void* c, const void* Tw, double out[5])
 {
-    CK(is64(ctx) ? launch_diag<double>(ctx->dd, phi, c, ctx->d_part, ctx->nblk, ctx->d_out, ctx->stream)
-                 : launch_diag<float>(ctx->dd, phi, c, ctx->d_part, ctx->nblk, ctx->d_out, ctx->stream),
+    const void* dp = ctx->fld[PF_DPP];
+    CK(is64(ctx) ? launch_diag<double>(ctx->dd, phi, c, Tw, dp, ctx->d_part, ctx->nblk, ctx->d_out, ctx->stream)
+                 : launch_diag<float>(ctx->dd, phi, c, Tw, dp, ctx->d_part, ctx->nblk, ctx->d_out, ctx->stream),
        "diagnosticos");
     CK(cudaMemcpyAsync(ctx->h_out, ctx->d_out, 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "diag copy");
     CK(cudaStreamSynchronize(ctx->stream), "diag sync");
@@ -474,14 +475,14 @@ static int run_diag(pf_ctx* ctx, const void* phi, const void* c, double out[5])
     if (rc != PF_OK) return rc;
     if (ctx->h_out[5] != 0.0)
         return ctx_err(ctx, PF_E_NONFINITE, "diagnosticos: " + std::to_string((long long)ctx->h_out[5]) +
-                                                " cells hold a non-finite phi or c (the run has blown up)");
+                                                " cells hold a non-finite phi, c, T or DPP (the run has blown up)");
     return PF_OK;
 }
 
 int pf_diagnosticos(pf_ctx* ctx, double out[5])
 {
     if (!ctx || !out) return PF_E_ARG;
-    return run_diag(ctx, ctx->fld[PF_PHASE_NEW], ctx->fld[PF_CONC_NEW], out);
+    return run_diag(ctx, ctx->fld[PF_PHASE_NEW], ctx->fld[PF_CONC_NEW], ctx->fld[PF_TNEW], out);
 }
 
 int pf_track(pf_ctx* ctx, double out[3])
@@ -786,7 +787,7 @@ int pf_step_diag(pf_ctx* ctx, int n_steps, double out[5])
     int rc = pf_step(ctx, n_steps);
     if (rc) return rc;
     // after the exchange the final state sits in the "old" buffers
-    return run_diag(ctx, ctx->fld[PF_PHASE_OLD], ctx->fld[PF_CONC_OLD], out);
+    return run_diag(ctx, ctx->fld[PF_PHASE_OLD], ctx->fld[PF_CONC_OLD], ctx->fld[PF_TOLD], out);
 }
 
 int pf_init_seeded(pf_ctx* ctx, int n_bumps, const double* sites)

@@ -86,6 +86,7 @@ struct pf_batch {
     int march = 1;                     // TMA-staged march passes (32 x 8 tiles); 0: the cp.async passes
     int nslot = 0;                     // node-window planes of the march passes (0: 3 in FP64, 4 in FP32)
     CUtensorMap* d_tmaps = nullptr;    // 2 per slot: the tensor maps of its phase-field buffers
+    int* d_ctr = nullptr;              // work-item counters of a graph's launches (2 per step)
     int* d_status = nullptr;           // kernel status word (0, or the code a kernel left there)
     cudaStream_t own_stream = nullptr, stream = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -193,6 +194,8 @@ static int capture_graph(pf_batch* b)
     BCK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "capture stream");
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess && march)   // the work counters of the graph's launches start at zero
+        e = cudaMemsetAsync(b->d_ctr, 0, 2 * kGraphSteps * sizeof(int), cs);
     if (e == cudaSuccess) {
         for (int k = 0; k < kGraphSteps && e == cudaSuccess; ++k) {
             const BatchStep* st = b->d_steps + (size_t)k * b->max_domains;
@@ -202,10 +205,10 @@ static int capture_graph(pf_batch* b)
                 for (int pass = 0; pass <= (one ? 0 : 1) && e == cudaSuccess; ++pass)
                     e = b64(b) ? launch_march_batch<double>(b->d_doms, b->d_tmaps, st, b->d_items, b->d_nitems, pass,
                                                             one, smooth && pass == 0, lanes, nslot, b->zchunk,
-                                                            b->n_sm, b->d_status, cs)
+                                                            b->n_sm, b->d_ctr + 2 * k + pass, b->d_status, cs)
                                : launch_march_batch<float>(b->d_doms, b->d_tmaps, st, b->d_items, b->d_nitems, pass,
                                                            one, smooth && pass == 0, lanes, nslot, b->zchunk,
-                                                           b->n_sm, b->d_status, cs);
+                                                           b->n_sm, b->d_ctr + 2 * k + pass, b->d_status, cs);
                 continue;
             }
             if (pair) {
@@ -335,6 +338,7 @@ int pf_batch_create(int precision, long long budget_bytes, int max_domains, pf_b
         (e = cudaMalloc(&b->d_sites, 2 * 4096 * sizeof(double))) != cudaSuccess ||
         (e = cudaMalloc(&b->d_tmaps, sizeof(CUtensorMap) * 2 * (size_t)max_domains)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_status, sizeof(int))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_ctr, 2 * kGraphSteps * sizeof(int))) != cudaSuccess ||
         (e = cudaMallocHost(&b->h_out, 8 * sizeof(double))) != cudaSuccess ||
         (e = cudaEventCreate(&b->h_ev[0])) != cudaSuccess || (e = cudaEventCreate(&b->h_ev[1])) != cudaSuccess ||
         (e = cudaEventCreate(&b->ev0)) != cudaSuccess || (e = cudaEventCreate(&b->ev1)) != cudaSuccess) {
@@ -382,6 +386,7 @@ int pf_batch_destroy(pf_batch* b)
     cudaFree(b->d_sites);
     cudaFree(b->d_tmaps);
     cudaFree(b->d_status);
+    cudaFree(b->d_ctr);
     cudaFreeHost(b->h_out);
     for (cudaEvent_t ev : {b->h_ev[0], b->h_ev[1], b->ev0, b->ev1})
         if (ev) cudaEventDestroy(ev);
@@ -870,9 +875,9 @@ int pf_batch_diagnosticos(pf_batch* b, int slot, double out[5])
     if (!sl || !out) return berr(b, PF_E_ARG, "pf_batch_diagnosticos: bad argument");
     double* res = b->d_part + 592 * kDiagRow;
     cudaError_t e = b64(b) ? launch_diag<double>(sl->bd.d, slot_field(*sl, PF_PHASE_OLD), slot_field(*sl, PF_CONC_OLD),
-                                                 b->d_part, 592, res, b->stream)
+                                                 slot_field(*sl, PF_TOLD), sl->bd.dpp, b->d_part, 592, res, b->stream)
                            : launch_diag<float>(sl->bd.d, slot_field(*sl, PF_PHASE_OLD), slot_field(*sl, PF_CONC_OLD),
-                                                b->d_part, 592, res, b->stream);
+                                                slot_field(*sl, PF_TOLD), sl->bd.dpp, b->d_part, 592, res, b->stream);
     BCK(e, "pf_batch_diagnosticos");
     BCK(cudaMemcpyAsync(b->h_out, res, 6 * sizeof(double), cudaMemcpyDeviceToHost, b->stream), "diag copy");
     BCK(cudaStreamSynchronize(b->stream), "diag sync");
@@ -881,7 +886,7 @@ int pf_batch_diagnosticos(pf_batch* b, int slot, double out[5])
     if (rc != PF_OK) return rc;
     if (b->h_out[5] != 0.0)
         return berr(b, PF_E_NONFINITE, "pf_batch_diagnosticos: " + std::to_string((long long)b->h_out[5]) +
-                                           " cells of the slot hold a non-finite phi or c (the run has blown up)");
+                                           " cells of the slot hold a non-finite phi, c, T or DPP (the run has blown up)");
     return PF_OK;
 }
 

@@ -14,7 +14,7 @@ template cudaError_t launch_solute<float>(const DomainDesc&, const StepArgs&, co
 template cudaError_t launch_copy_inner<float>(const DomainDesc&, const void*, void*, cudaStream_t);
 template cudaError_t launch_fused_first<float>(const DomainDesc&, const StepArgs&, const Fields&, bool, int, int, cudaStream_t);
 template cudaError_t launch_fused_last<float>(const DomainDesc&, const StepArgs&, const Fields&, int, int, cudaStream_t);
-template cudaError_t launch_diag<float>(const DomainDesc&, const void*, const void*, double*, int, double*, cudaStream_t);
+template cudaError_t launch_diag<float>(const DomainDesc&, const void*, const void*, const void*, const void*, double*, int, double*, cudaStream_t);
 template cudaError_t launch_convert_in<float>(const DomainDesc&, const double*, void*, long long, long long, cudaStream_t);
 template cudaError_t launch_convert_out<float>(const DomainDesc&, const void*, double*, long long, long long, cudaStream_t);
 template cudaError_t launch_fused_batch<float>(const BatchDomain*, const BatchStep*, const BatchItem*, const int*, int, bool, bool, int, int, int, cudaStream_t);

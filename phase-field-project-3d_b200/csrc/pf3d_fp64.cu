@@ -12,7 +12,7 @@ template cudaError_t launch_heat<double>(const DomainDesc&, const StepArgs&, con
 template cudaError_t launch_phase<double>(const DomainDesc&, const StepArgs&, const void*, const void*, void*, void*, cudaStream_t);
 template cudaError_t launch_solute<double>(const DomainDesc&, const StepArgs&, const void*, const void*, void*, cudaStream_t);
 template cudaError_t launch_copy_inner<double>(const DomainDesc&, const void*, void*, cudaStream_t);
-template cudaError_t launch_diag<double>(const DomainDesc&, const void*, const void*, double*, int, double*, cudaStream_t);
+template cudaError_t launch_diag<double>(const DomainDesc&, const void*, const void*, const void*, const void*, double*, int, double*, cudaStream_t);
 template cudaError_t launch_convert_in<double>(const DomainDesc&, const double*, void*, long long, long long, cudaStream_t);
 template cudaError_t launch_convert_out<double>(const DomainDesc&, const void*, double*, long long, long long, cudaStream_t);
 template <>

@@ -86,12 +86,12 @@ template <typename S> cudaError_t launch_march_last(const CUtensorMap& tm, const
                                                     const Fields& f, int lanes, int nslot, int zchunk, int* err,
                                                     cudaStream_t st);
 // batch form: tmaps[2 d + b] is the tensor map of buffer b of domain d's
-// phase field
+// phase field; *ctr (zero before the launch) hands out the work items
 template <typename S> cudaError_t launch_march_batch(const BatchDomain* doms, const CUtensorMap* tmaps,
                                                      const BatchStep* steps, const BatchItem* items,
                                                      const int* n_items, int pass, bool one_sweep, bool smooth,
-                                                     int lanes, int nslot, int zchunk, int n_sm, int* err,
-                                                     cudaStream_t st);
+                                                     int lanes, int nslot, int zchunk, int n_sm, int* ctr,
+                                                     int* err, cudaStream_t st);
 
 // Solidification tracking of phi: out[3] = {solid fraction, tip position
 // (cells, 1-based), solid cells}; scratch holds nz + 1 words.
@@ -108,8 +108,10 @@ template <typename T> cudaError_t launch_fill(void* a, long long n, double v, cu
 // the five values of diagnosticos and the count of cells whose phi or c is
 // not finite (the watchdog).
 constexpr int kDiagRow = 10;   // l2, l2 comp, max, min, sol, sol comp, fe, fe comp, non-finite cells, pad
-template <typename T> cudaError_t launch_diag(const DomainDesc& d, const void* phi, const void* c, double* part,
-                                              int nblk, double* out, cudaStream_t st);
+// Tw and dpp (may be null): the temperature and DPP fields the watchdog
+// also checks for non-finite values.
+template <typename T> cudaError_t launch_diag(const DomainDesc& d, const void* phi, const void* c, const void* Tw,
+                                              const void* dppw, double* part, int nblk, double* out, cudaStream_t st);
 
 // FP64 host array (Fortran order, nx*ny*nz) <-> pitched device field of T,
 // through a device staging buffer of doubles (FP32 contexts only).

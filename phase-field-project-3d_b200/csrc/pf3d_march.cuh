@@ -716,16 +716,21 @@ __global__ void __launch_bounds__(32 * TY / L, (MarchOcc<S, L, WIN, SOL, HEAT, S
 // many domains: a persistent grid walks the work list.  PASS 0 is the first
 // pass of a step (temperatura + sweep 1, or the whole step with one sweep),
 // PASS 1 the last (sweep 2 + solute).  tmaps[2 d + b] describes buffer b of
-// domain d's phase field.
+// domain d's phase field.  Items are handed out dynamically: each CTA starts
+// with item blockIdx.x and then takes the next unclaimed item from the
+// counter *ctr (zero before the launch), so CTAs that drew short items (thin
+// z-chunks, small domains at the end of the largest-first list) keep
+// working while others finish long ones.
 template <typename S, int L, int TY, int WIN, int PASS, bool ONE_SWEEP, bool SMOOTH>
 __global__ void __launch_bounds__(32 * TY / L,
                                   (MarchOcc<S, L, WIN, PASS == 1 || ONE_SWEEP, PASS == 0, SMOOTH>::v))
     k_march_batch(const BatchDomain* __restrict__ doms, const CUtensorMap* __restrict__ tmaps,
                   const BatchStep* __restrict__ steps, const BatchItem* __restrict__ items,
-                  const int* __restrict__ n_items, int zchunk, int* __restrict__ err)
+                  const int* __restrict__ n_items, int zchunk, int* __restrict__ ctr, int* __restrict__ err)
 {
     using V = typename Lanes<S, L>::V;
     constexpr bool SOL = PASS == 1 || ONE_SWEEP;
+    __shared__ int s_next;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(16) KC<S> skc;   // the loop constants of the current item
     __shared__ __align__(16) KC<V> skv;   // the same, broadcast to the lanes (L = 2)
@@ -736,10 +741,17 @@ __global__ void __launch_bounds__(32 * TY / L,
     uint32_t par = 0;
     const int n = *n_items;
     const int tid = threadIdx.x + 32 * threadIdx.y;
-    for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    for (int w = blockIdx.x; w < n;) {
         const BatchItem it = items[w];
         const BatchStep& st = steps[it.dom];
-        if (!st.active) continue;   // uniform across the CTA
+        // the next item, claimed now so the atomic's latency hides behind this one
+        __syncthreads();            // every thread has read the previous claim
+        if (tid == 0) s_next = (int)gridDim.x + atomicAdd(ctr, 1);
+        if (!st.active) {           // uniform across the CTA
+            __syncthreads();
+            w = s_next;
+            continue;
+        }
         const BatchDomain& D = doms[it.dom];
         const int q = st.q_phi, qc = st.q_c, qt = st.q_T;
         __syncthreads();            // the previous item is done with the constants and the windows
@@ -780,6 +792,8 @@ __global__ void __launch_bounds__(32 * TY / L,
             if (tid == 0) atomicExch(err, kErrTmaTimeout);
             return;
         }
+        __syncthreads();            // the claim is visible (and the tile is done)
+        w = s_next;
     }
 }
 
@@ -869,8 +883,8 @@ cudaError_t launch_march_last(const CUtensorMap& tm, const DomainDesc& d, const 
 // resident on one SM.
 template <typename S, int L, int WIN, int PASS, bool ONE_SWEEP, bool SMOOTH>
 cudaError_t launch_march_batch_t(const BatchDomain* doms, const CUtensorMap* tmaps, const BatchStep* steps,
-                                 const BatchItem* items, const int* n_items, int zchunk, int n_sm, int* err,
-                                 cudaStream_t st)
+                                 const BatchItem* items, const int* n_items, int zchunk, int n_sm, int* ctr,
+                                 int* err, cudaStream_t st)
 {
     constexpr bool SOL = PASS == 1 || ONE_SWEEP;
     using LY = MarchLayout<S, 8, SOL, MarchWin<WIN>::nslot>;
@@ -884,17 +898,17 @@ cudaError_t launch_march_batch_t(const BatchDomain* doms, const CUtensorMap* tma
         if (e != cudaSuccess) return e;
         per_sm = nb > 0 ? nb : 1;
     }
-    kern<<<n_sm * per_sm, dim3(32, 8 / L), LY::ALLOC, st>>>(doms, tmaps, steps, items, n_items, zchunk, err);
+    kern<<<n_sm * per_sm, dim3(32, 8 / L), LY::ALLOC, st>>>(doms, tmaps, steps, items, n_items, zchunk, ctr, err);
     return cudaGetLastError();
 }
 
 template <typename S>
 cudaError_t launch_march_batch(const BatchDomain* doms, const CUtensorMap* tmaps, const BatchStep* steps,
                                const BatchItem* items, const int* n_items, int pass, bool one_sweep, bool smooth,
-                               int lanes, int win, int zchunk, int n_sm, int* err, cudaStream_t st)
+                               int lanes, int win, int zchunk, int n_sm, int* ctr, int* err, cudaStream_t st)
 {
 #define PF3D_MB(L, NS, P, ONE, SM) \
-    launch_march_batch_t<S, L, NS, P, ONE, SM>(doms, tmaps, steps, items, n_items, zchunk, n_sm, err, st)
+    launch_march_batch_t<S, L, NS, P, ONE, SM>(doms, tmaps, steps, items, n_items, zchunk, n_sm, ctr, err, st)
 #define PF3D_MW(L, P, ONE, SM) \
     (win == 3 ? PF3D_MB(L, 3, P, ONE, SM) : win == 4 ? PF3D_MB(L, 4, P, ONE, SM) : PF3D_MB(L, 5, P, ONE, SM))
     if (pass == 0) {

@@ -3,5 +3,5 @@
 #include "pf3d_march.cuh"
 
 namespace pf3d {
-template cudaError_t launch_march_batch<double>(const BatchDomain*, const CUtensorMap*, const BatchStep*, const BatchItem*, const int*, int, bool, bool, int, int, int, int, int*, cudaStream_t);
+template cudaError_t launch_march_batch<double>(const BatchDomain*, const CUtensorMap*, const BatchStep*, const BatchItem*, const int*, int, bool, bool, int, int, int, int, int*, int*, cudaStream_t);
 }  // namespace pf3d

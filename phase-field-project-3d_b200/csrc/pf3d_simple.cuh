@@ -144,8 +144,10 @@ __global__ void __launch_bounds__(256) k_copy_inner(DomainDesc d, const T* __res
 // ---- diagnosticos.f90 + diag_body.inc ----
 // FP64 accumulation with Neumaier compensation; max/min exact and NaN-
 // propagating (fmax/fmin would drop a NaN and report finite extremes for a
-// blown-up field); plus the watchdog: the count of cells whose phi or c is
-// not finite.  Partials: kDiagRow doubles per block (pf3d_launch.h).
+// blown-up field); plus the watchdog: the count of cells where phi, c, or
+// (when given) T or DPP is not finite.  The clamp of the phase update maps a
+// NaN or infinite update to 1, so a blow-up can leave phi finite and show
+// only in DPP and T.  Partials: kDiagRow doubles per block (pf3d_launch.h).
 
 // max / min that return NaN when either argument is NaN
 __device__ __forceinline__ double nan_max(double a, double b) { return (a > b || a != a) ? a : b; }
@@ -168,6 +170,7 @@ struct KSum {
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_diag(DomainDesc d, const T* __restrict__ pn, const T* __restrict__ cn,
+                                              const T* __restrict__ tw, const T* __restrict__ dw,
                                               double* __restrict__ part)
 {
     const long long ncell = (long long)d.nx * d.ny * d.nz;
@@ -186,7 +189,10 @@ __global__ void __launch_bounds__(256) k_diag(DomainDesc d, const T* __restrict_
         mx = nan_max(mx, phi);
         mn = nan_min(mn, phi);
         sol.add(cv);
-        if (!isfinite(phi) || !isfinite(cv)) bad += 1.0;
+        bool fin = isfinite(phi) && isfinite(cv);
+        if (tw) fin = fin && isfinite((double)tw[id]);
+        if (dw) fin = fin && isfinite((double)dw[id]);
+        if (!fin) bad += 1.0;
         double w_term = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(w0, phi), phi), 1.0 - phi), 1.0 - phi);
         double grad2 = 0.0;
         if (x > 0 && x < d.nx - 1 && y > 0 && y < d.ny - 1 && z > 0 && z < d.nz - 1) {
@@ -313,10 +319,10 @@ cudaError_t launch_copy_inner(const DomainDesc& d, const void* src, void* dst, c
 }
 
 template <typename T>
-cudaError_t launch_diag(const DomainDesc& d, const void* phi, const void* c, double* part, int nblk, double* out,
-                        cudaStream_t st)
+cudaError_t launch_diag(const DomainDesc& d, const void* phi, const void* c, const void* Tw, const void* dppw,
+                        double* part, int nblk, double* out, cudaStream_t st)
 {
-    k_diag<T><<<nblk, 256, 0, st>>>(d, (const T*)phi, (const T*)c, part);
+    k_diag<T><<<nblk, 256, 0, st>>>(d, (const T*)phi, (const T*)c, (const T*)Tw, (const T*)dppw, part);
     k_diag_final<T><<<1, 32, 0, st>>>(part, nblk, out);
     return cudaGetLastError();
 }

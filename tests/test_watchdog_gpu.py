@@ -5,8 +5,10 @@ uploaded field (nothing faults, traps or hangs the GPU).  The diagnostics
 then return PF_E_NONFINITE with max/min propagated as NaN (fmax/fmin would
 have dropped the NaN and reported finite extremes), for a single domain,
 for the fused step with diagnostics, and for a batch slot; the server
-retires such a request as failed instead of returning its numbers.  A finite
-state still reports success with the same values as before."""
+retires such a request as failed instead of returning its numbers.  The
+phase update's clamp turns a NaN or infinite update into 1, so after a step
+a blow-up may show only in DPP and T: the watchdog counts those fields too.
+A finite state still reports success with the same values as before."""
 import math
 
 import numpy as np
