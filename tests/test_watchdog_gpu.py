@@ -8,7 +8,10 @@ for the fused step with diagnostics, and for a batch slot; the server
 retires such a request as failed instead of returning its numbers.  The
 phase update's clamp turns a NaN or infinite update into 1, so after a step
 a blow-up may show only in DPP and T: the watchdog counts those fields too.
-A finite state still reports success with the same values as before."""
+A NaN written into phi is therefore absorbed within a step or two (the cell
+becomes solid, the heat equation's interior update does not read TOLD); a
+NaN in c is not clamped and spreads, so the stepped cases poison c.  A
+finite state still reports success with the same values as before."""
 import math
 
 import numpy as np
@@ -68,6 +71,21 @@ def test_max_min_propagate_nan(gpu):
         assert math.isfinite(out[3])   # the solute total does not read phi
 
 
+def test_a_nan_in_phi_is_absorbed_by_the_clamp(gpu):
+    """The reference's clamp dmax1(0, dmin1(1, .)) maps a NaN update to 1:
+    a NaN written into phi leaves, after two steps, a finite state (the
+    watchdog rightly reports nothing)."""
+    g, p, st = case()
+    st = dict(st)
+    st["phi"] = st["phi"].copy()
+    st["phi"][9, 10, 11] = np.nan
+    with pf3d.Domain(g, p, pf3d.PF_FP64) as d:
+        d.load_state(st)
+        out = d.step_diag(2)
+        assert all(math.isfinite(v) for v in out)
+        assert d.download("phase_field_old")[9, 10, 11] > 0.5   # the cell turned solid
+
+
 def test_step_diag_reports_a_blown_up_state(gpu):
     g, p, st = case()
     st = dict(st)
@@ -96,7 +114,15 @@ def test_batch_diagnosticos_flag_the_bad_slot_only(gpu, prec):
         b.load_state(a, s1)
         c = b.add(g2, p2)
         b.load_state(c, s2)
-        b.step(2)
+        assert all(math.isfinite(v) for v in b.diagnosticos(a))
+        with pytest.raises(pf3d.PFError) as e:   # as uploaded
+            b.diagnosticos(c)
+        assert e.value.code == pf3d.PF_E_NONFINITE
+        s2["phi"][10, 11, 12] = s1["phi"][0, 0, 0]
+        s2["c"] = s2["c"].copy()
+        s2["c"][10, 11, 12] = np.inf
+        b.load_state(c, s2)
+        b.step(2)                                  # a c that is not finite spreads
         out = b.diagnosticos(a)
         assert all(math.isfinite(v) for v in out)
         with pytest.raises(pf3d.PFError) as e:
@@ -116,13 +142,13 @@ def test_server_retires_a_blown_up_request_as_failed(gpu):
     victim = jobs[1]
 
     def poison(srv, done, waiting):
-        # after the first quantum, write a NaN into the victim's phase field
+        # after the first quantum, write a NaN into the victim's concentration
         prec = victim.precision
         if victim.slot >= 0 and victim.slot in srv.active[prec] and not getattr(poison, "done", False):
             b = srv.batches[prec]
-            phi = b.download(victim.slot, "phase_field_old")
-            phi[20, 16, 16] = np.nan
-            b.upload(victim.slot, "phase_field_old", phi)
+            c = b.download(victim.slot, "conc_soluto_old")
+            c[20, 16, 16] = np.nan
+            b.upload(victim.slot, "conc_soluto_old", c)
             poison.done = True
 
     srv = serve.Server(budget_bytes=8e9, quantum=8)
