@@ -691,7 +691,7 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
 template <typename S, int L, int WIN, bool SOL, bool HEAT, bool SMOOTH = false>
 struct MarchOcc {
     static constexpr int v = (sizeof(S) == 8) ? ((WIN == 5 || (SOL && WIN == 4) || SMOOTH) ? 2 : 3)
-                                              : (L == 2 ? ((HEAT && WIN != 5) ? 5 : 4) : 3);
+                                              : (L == 2 ? ((HEAT && WIN != 5) ? 6 : 5) : 3);
 };
 
 // single domain: one CTA per tile; the phase field comes through `tm`
