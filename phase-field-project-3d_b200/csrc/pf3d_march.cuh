@@ -32,6 +32,7 @@
 // the step's REAL(4) noise in the DPP buffer and the last pass reads it back
 // (both sweeps use the same it, so the same noise: principal.f90:127-151).
 #pragma once
+#include <type_traits>
 #include "pf3d_launch.h"
 #include "pf3d_pair.cuh"
 #include "pf3d_tma.cuh"
@@ -142,8 +143,10 @@ __device__ __forceinline__ void march_init_barriers(unsigned char* smem)
 // from the phase field the tensor map `tm` describes.  `par` carries the
 // parity of each plane barrier across the tiles a CTA processes (every load
 // issued is waited for).  Returns false if a plane load did not arrive in
-// time; the CTA must then stop.
-template <typename S, int L, int TY, int WIN, bool HEAT, bool DPPW, bool SOL, bool SMOOTH>
+// time; the CTA must then stop.  SPLIT: a second copy of the plane body for
+// the interior planes, without their z checks (single domains; a batch's
+// short items gain less than the larger code costs them, measured).
+template <typename S, int L, int TY, int WIN, bool HEAT, bool DPPW, bool SOL, bool SMOOTH, bool SPLIT = true>
 __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, const KC<typename Lanes<S, L>::V>& cv,
                                            const CUtensorMap* tm, const S* __restrict__ c_in,
                                            S* __restrict__ phi_out, S* __restrict__ dpp, S* __restrict__ c_out,
@@ -414,7 +417,15 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
     int s6 = zb % 6;       // phase slot of plane z
     int sn = zb % NSLOT;   // node / point slot of plane z
 
-    for (int z = zb; z < ze; ++z, zoff += pl) {
+    // One plane of the march.  IN: every z-dependent condition of the plane
+    // is known true (z in [3, N-4], the planes it reads and the load it
+    // issues all inside the domain and the chunk), so that copy of the body
+    // carries none of the checks; the other copy serves the first and last
+    // planes.  Returns false when a plane load did not arrive.  Always
+    // inlined: an outlined copy would pass every captured value through the
+    // stack (measured: 5x slower).
+    auto plane = [&](int z, auto in_tag) __attribute__((always_inline)) -> bool {
+        constexpr bool IN = decltype(in_tag)::value;
         const int s6p1 = wrap_add<6>(s6, 1), s6p2 = wrap_add<6>(s6, 2);
         const int snm1 = wrap_add<NSLOT>(sn, NSLOT - 1), snp1 = wrap_add<NSLOT>(sn, 1);
         const S* const pm = sphi + wrap_add<6>(s6, 5) * LY::PHI_SLOT;
@@ -429,11 +440,11 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
         else load_c(z + 1, co[1], cr[1]);
 
         // A: plane z+2 has landed
-        if (z + 2 <= zlast) bad |= !wait_plane(s6p2);
+        if (IN || z + 2 <= zlast) bad |= !wait_plane(s6p2);
         // B, C: nodes and solute points of plane z+1
         if constexpr (ROLL) {
             load5(rpp, pp);   // plane z+1 at the own column: the stencil's T values and the node's x/y gradient
-            if (z + 1 >= 1 && z + 1 <= nz - 2) {
+            if (IN || (z + 1 >= 1 && z + 1 <= nz - 2)) {
                 S a[L], b[L];
 #pragma unroll
                 for (int l = 0; l < L; ++l) { a[l] = rpp[l][3]; b[l] = rpp[l][4]; }
@@ -459,15 +470,15 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
                     node_store(dst, rnode_off, rx, ry, rz, nullptr);
                 }
             }
-            if (SOL && z + 1 <= nz - 1) {
+            if (SOL && (IN || z + 1 <= nz - 1)) {
                 S op[L];
 #pragma unroll
                 for (int l = 0; l < L; ++l) op[l] = rpp[l][0];
                 sol_plane(snp1, pp, co[1], cr[0], rsT, op);
             }
         } else {
-            if (z + 1 >= 1 && z + 1 <= nz - 2) node_plane(snp1, p0, pp, pq, nullptr);
-            if (SOL && z + 1 <= nz - 1) sol_plane(snp1, pp, co[1], cr[0], nullptr, nullptr);
+            if (IN || (z + 1 >= 1 && z + 1 <= nz - 2)) node_plane(snp1, p0, pp, pq, nullptr);
+            if (SOL && (IN || z + 1 <= nz - 1)) sol_plane(snp1, pp, co[1], cr[0], nullptr, nullptr);
         }
         // D: one barrier orders the plane; everyone learns of a failed load
         if (__syncthreads_or(bad)) {
@@ -475,14 +486,14 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
             return false;
         }
         // E: the load of plane z+4 into the slot plane z-2 has left
-        if (lead && z + 4 <= zlast) {
+        if (lead && (IN || z + 4 <= zlast)) {
             fence_proxy_async_smem();
             issue(z + 4, wrap_add<6>(s6, 4));
         }
 
         // F: the cells of plane z
-        const bool zin = z >= 1 && z <= nz - 2;   // T interior / phase source / solute interior
-        const bool zph = z >= 2 && z <= nz - 3;   // phase interior
+        const bool zin = IN || (z >= 1 && z <= nz - 2);   // T interior / phase source / solute interior
+        const bool zph = IN || (z >= 2 && z <= nz - 3);   // phase interior
         const S* const nm1 = snode + snm1 * LY::NODE_SLOT;
         const S* const n0 = snode + sn * LY::NODE_SLOT;
         const S* const np1 = snode + snp1 * LY::NODE_SLOT;
@@ -587,7 +598,7 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
         const V U = clamp01(ppn);
         const V DP = ppn - PP;
 
-        if (tile_int && z >= 3 && z <= nz - 4) {
+        if (tile_int && (IN || (z >= 3 && z <= nz - 4))) {
             // every cell of the tile plane is interior and its own only
             // preimage (CTA-uniform branch)
 #pragma unroll
@@ -678,6 +689,22 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
         sn = snp1;
         // window mode 3: the next plane's nodes overwrite plane z-1's slot
         if constexpr (MarchWin<WIN>::two_barriers) __syncthreads();
+            zoff += pl;
+        return true;
+    };
+    if constexpr (SPLIT) {
+        // interior planes [zi0, zi1): z >= 3, z <= nz - 4 and z + 4 <= zlast
+        const int zi0 = max(zb, 3), zi1 = min(min(ze, nz - 3), zlast - 3);
+        int z = zb;
+        for (; z < ze && z < zi0; ++z)
+            if (!plane(z, std::false_type{})) return false;
+        for (; z < zi1; ++z)
+            if (!plane(z, std::true_type{})) return false;
+        for (; z < ze; ++z)
+            if (!plane(z, std::false_type{})) return false;
+    } else {
+        for (int z = zb; z < ze; ++z)
+            if (!plane(z, std::false_type{})) return false;
     }
     return true;
 }
@@ -775,16 +802,16 @@ __global__ void __launch_bounds__(32 * TY / L,
         if (PASS == 0) {
             const CUtensorMap* tm = tmaps + 2 * it.dom + q;
             if (ONE_SWEEP)
-                ok = march_tile<S, L, TY, WIN, true, true, true, SMOOTH>(
+                ok = march_tile<S, L, TY, WIN, true, true, true, SMOOTH, false>(
                     D.d, skc, kv, tm, (const S*)D.c[qc], (S*)D.phi[1 - q], (S*)D.dpp, (S*)D.c[1 - qc],
                     (const S*)D.T[qt], (S*)D.T[1 - qt], zchunk, it.bx, it.by, it.bz, smem, par);
             else
-                ok = march_tile<S, L, TY, WIN, true, false, false, SMOOTH>(
+                ok = march_tile<S, L, TY, WIN, true, false, false, SMOOTH, false>(
                     D.d, skc, kv, tm, (const S*)D.c[qc], (S*)D.phi[1 - q], (S*)D.dpp, nullptr, (const S*)D.T[qt],
                     (S*)D.T[1 - qt], zchunk, it.bx, it.by, it.bz, smem, par);
         } else {
             const CUtensorMap* tm = tmaps + 2 * it.dom + (1 - q);
-            ok = march_tile<S, L, TY, WIN, false, true, true, false>(
+            ok = march_tile<S, L, TY, WIN, false, true, true, false, false>(
                 D.d, skc, kv, tm, (const S*)D.c[qc], (S*)D.phi[q], (S*)D.dpp, (S*)D.c[1 - qc], nullptr, nullptr,
                 zchunk, it.bx, it.by, it.bz, smem, par);
         }
