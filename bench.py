@@ -210,9 +210,15 @@ def bench_fp32(args, torch, pf3d, deck, init, stream, world):
             "hbm_frac_step": v / world * STEP_BYTES_PER_CELL[32] / peak, "init": "device (pf_init_seeded)"}
 
 
-def bench_batch(args, pf3d, serve, init):
-    """96 FP32 domains of uneven size (configuration 4), autotuned tiles."""
-    jobs = serve.batch_domains(seed=3)
+def bench_batch(args, pf3d, serve, init, world=1, rank=0, barrier=None, max_over_ranks=None):
+    """96 FP32 domains of uneven size (configuration 4), autotuned tiles.
+    With N ranks the domains are routed longest-first (replicas.assign on
+    their cells) and every rank runs its share as one batch; the same 96
+    domains in total, so the scaling is strong, timed as the slowest rank."""
+    from pf3d import replicas
+    jobs_all = serve.batch_domains(seed=3)
+    costs = [j.cells for j in jobs_all]
+    jobs = [jobs_all[i] for i in replicas.my_share(costs, world, rank)]
     b = pf3d.Batch(pf3d.PF_FP32)
     for j in jobs:
         s = b.add(j.grid(), j.params())
@@ -223,12 +229,21 @@ def bench_batch(args, pf3d, serve, init):
     tune_s = time.perf_counter() - t0
     b.step(8)
     n = max(16, args.steps)
+    if barrier:
+        barrier()
     ms = b.step(n)
-    cells = sum(j.cells for j in jobs)
+    if max_over_ranks:
+        ms = max_over_ranks(ms)
+    cells = sum(costs)
     b.close()
-    return {"workload": "c4_96_domains_fp32", "domains": len(jobs), "cells": cells, "steps": n,
-            "ms_per_step": ms / n, "value": cells * n / (ms / 1e3) / 1e9, "unit": UNIT,
-            "tile": [32, ty, zc], "autotune_s": tune_s, "launch": "persistent work-list kernels, CUDA graph of 8 steps"}
+    out = {"workload": "c4_96_domains_fp32", "domains": len(jobs_all), "cells": cells, "steps": n,
+           "ms_per_step": ms / n, "value": cells * n / (ms / 1e3) / 1e9, "unit": UNIT,
+           "tile": [32, ty, zc], "autotune_s": tune_s, "launch": "persistent work-list kernels, CUDA graph of 8 steps"}
+    if world > 1:
+        out["scaling"] = "strong"
+        out["routing"] = "longest-first on cells; rank 0 holds %d domains, %.1f M cells" % (
+            len(jobs), sum(j.cells for j in jobs) / 1e6)
+    return out
 
 
 def bench_karma(args, torch, stream):
@@ -467,10 +482,10 @@ def main():
     if not args.no_fp32:
         extra["fp32"] = bench_fp32(args, torch, pf3d, deck, init, stream, world)
         extra["fp32"]["speedup_vs_fp64"] = extra["fp32"]["value"] / value
+    from pf3d import serve as serve_mod
+    if not args.no_batch:   # every rank: the 96 domains are spread over the ranks
+        extra["batched"] = bench_batch(args, pf3d, serve_mod, init, world, rank, barrier, max_over_ranks)
     if rank == 0 and world == 1:
-        from pf3d import serve as serve_mod
-        if not args.no_batch:
-            extra["batched"] = bench_batch(args, pf3d, serve_mod, init)
         if not args.no_error:
             extra["fp32_error"] = bench_fp32_error(args)
         if not args.no_serve:

@@ -56,3 +56,18 @@ def test_two_ranks_gloo():
     assert all(r[3] == 2.0 for r in res)                    # MAX over ranks
     assert sorted(res[0][4] + res[1][4]) == list(range(6))  # every domain exactly once
     assert all(abs(r[5] - 10.0) < 1e-12 for r in res)       # 2 ranks x 1e9 x 10 / 2 s
+
+
+@pytest.mark.parametrize("world", [2, 4, 8])
+def test_batched_domains_routing(world):
+    """The batched workload's 96 domains spread over N ranks (bench.py's
+    batched sub-line at N > 1): every domain on exactly one rank, and the
+    slowest rank's cells within LPT's 4/3 of the lower bound max(total/N,
+    largest domain)."""
+    from pf3d import serve
+    costs = [j.cells for j in serve.batch_domains(seed=3)]
+    shares = [replicas.my_share(costs, world, r) for r in range(world)]
+    assert sorted(sum(shares, [])) == list(range(len(costs)))
+    worst = max(sum(costs[i] for i in s) for s in shares)
+    bound = max(sum(costs) / world, max(costs))
+    assert worst <= 4 / 3 * bound
