@@ -443,6 +443,22 @@ def main():
                 "ncu_figures": fig}
     step_hbm_frac = step_gbs / peak
 
+    # ---- the diagnostics reduction (a separate pass, run at output events):
+    # its cost beside a step, from CUDA events around pf_diagnosticos ----
+    dom.diagnosticos()
+    torch.cuda.synchronize()
+    dms = []
+    for _ in range(3):
+        d0, d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        d0.record(stream)
+        dom.diagnosticos()
+        d1.record(stream)
+        torch.cuda.synchronize()
+        dms.append(d0.elapsed_time(d1))
+    diag = {"ms": min(dms), "alg_bytes_per_cell": 4 * (8 if prec == 64 else 4),
+            "frac_of_step": min(dms) / (ms / args.steps),
+            "reads": "phi, c, T, DPP (sums, extremes, free energy, non-finite count)"}
+
     # ---- end to end through the C-ABI with pinned host buffers ----
     e2e = None
     if not args.no_e2e:
@@ -514,6 +530,7 @@ def main():
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": launches_per_step * args.steps,
+        "diagnostics": diag,
         "clocks": clk,
     }
     line.update(extra)

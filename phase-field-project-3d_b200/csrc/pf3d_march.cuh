@@ -193,17 +193,23 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
         phi_off[l] = (ty + l * TR + 2) * TW + (tx + XOFF);
         node_off[l] = (ty + l * TR + 1) * NW + (tx + 1);
     }
-    // ---- the ring items of this thread: node-tile positions ----
+    // ---- the ring items of this thread: node-tile positions.  The first
+    // NRING threads compute the ring's node quantities, the last NRING its
+    // solute points (solute passes), so that no warp carries both ring parts
+    // of a plane while the others wait for it at the plane's barrier ----
+    constexpr int NT = 32 * TY / L;
+    static_assert(2 * NRING <= NT, "the node and solute ring threads are disjoint");
     int rlx[L], rly[L];
-    const bool ring = tid < NRING;
+    const bool ring = tid < NRING;                      // ring nodes
+    const bool ring_s = SOL && tid >= NT - NRING;       // ring solute points
     if (L == 1) {
-        int r = ring ? tid : 0;
+        int r = ring ? tid : (ring_s ? tid - (NT - NRING) : 0);
         if (r < NW) { rlx[0] = r; rly[0] = 0; }
         else if ((r -= NW) < NW) { rlx[0] = r; rly[0] = NH - 1; }
         else if ((r -= NW) < TY) { rlx[0] = 0; rly[0] = 1 + r; }
         else { r -= TY; rlx[0] = NW - 1; rly[0] = 1 + r; }
     } else {
-        const int r = ring ? tid : 0;
+        const int r = ring ? tid : (ring_s ? tid - (NT - NRING) : 0);
         if (r < NW) { rlx[0] = r; rly[0] = 0; rlx[L - 1] = r; rly[L - 1] = NH - 1; }
         else { rlx[0] = 0; rly[0] = 1 + (r - NW); rlx[L - 1] = NW - 1; rly[L - 1] = 1 + (r - NW); }
     }
@@ -213,7 +219,7 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
 #pragma unroll
     for (int l = 0; l < L; ++l) {
         const int gx = x0 - 1 + rlx[l], gy = y0 - 1 + rly[l];
-        rin[l] = ring && gx >= 0 && gx < nx && gy >= 0 && gy < ny;
+        rin[l] = ring_s && gx >= 0 && gx < nx && gy >= 0 && gy < ny;   // a ring point's concentration is read
         rcol[l] = (long long)gx + (long long)gy * px;
         rphi_off[l] = (rly[l] + 1) * TW + (rlx[l] - 1 + XOFF);
         rnode_off[l] = rly[l] * NW + rlx[l];
@@ -306,7 +312,7 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
             }
         };
         one(phi_off, node_off, co, keep, ownp);
-        if (ring) one(rphi_off, rnode_off, cr, nullptr, nullptr);
+        if (ring_s) one(rphi_off, rnode_off, cr, nullptr, nullptr);
     };
     // concentration of plane s at the own and ring points (a benign value
     // outside the domain, so that no logarithm there leaves the normal range)
