@@ -154,11 +154,10 @@ int pf_set_stream(pf_ctx* ctx, void* stream);
                               arithmetic with fan-out boundary stores; 0 the
                               element-wise cp.async passes.  Same results.  */
 #define PF_OPT_NSLOT 7     /* window mode of the TMA passes: 3 (3-plane
-                              node windows, two barriers a plane), 4 (4-plane
-                              windows, one barrier) or 5 (the own column's
-                              values carried in registers along z, 3-plane
-                              windows, one barrier); 0 (default) = the
-                              precision's measured best.  Same results.     */
+                              node windows), 4 (4-plane windows) or 5 (the
+                              own column's values carried in registers along
+                              z, 3-plane windows); one barrier a plane in
+                              each; 0 (default) = 3.  Same results.         */
 int pf_set_option(pf_ctx* ctx, int opt, int value);
 int pf_get_option(const pf_ctx* ctx, int opt, int* value);
 /* With PF_OPT_KTIMING on: launches and summed device milliseconds of the
@@ -328,7 +327,7 @@ int pf_batch_set_tile(pf_batch* b, int tile_y, int zchunk);
 int pf_batch_set_paired(pf_batch* b, int paired);
 /* Which fused passes a batch runs (same results): kernel 1 (default) the
    TMA-staged passes on 32 x 8 tiles, 0 the element-wise cp.async passes;
-   nslot as PF_OPT_NSLOT (0 = per precision)                               */
+   nslot as PF_OPT_NSLOT (0 = 3)                                           */
 int pf_batch_set_kernel(pf_batch* b, int kernel, int nslot);
 /* Autotuner: times every tile shape x z-chunk (16, 32, 64, 128) x one or
    two cells per thread -- tile heights 4, 8 and 16 for the cp.async passes,

@@ -72,7 +72,7 @@ struct pf_ctx {
     cudaStream_t stream;
     int fused, tile_y, zchunk, ktiming, paired;
     int kernel;              // PF_OPT_KERNEL: 1 TMA-staged march passes, 0 the cp.async passes
-    int nslot;               // PF_OPT_NSLOT: node-window planes of the march passes (0: per precision)
+    int nslot;               // PF_OPT_NSLOT: window mode of the march passes (0: 3)
     CUtensorMap tmap[2];     // tensor maps of the two phase-field buffers (32 x 8 march tiles)
     void* tmap_buf[2];       // their base addresses
     int tmap_ok;
@@ -649,11 +649,7 @@ static int one_step(pf_ctx* ctx)
         // TMA-staged passes: two cells per thread unless PF_OPT_PAIRED says
         // otherwise (default: FP32 only) or the deck draws the smooth noise
         const int lanes = ((ctx->paired == 2 || (ctx->paired == 1 && !is64(ctx))) && p.ruido_tipo != 2) ? 2 : 1;
-        // default window modes, measured per pass: FP32 4-plane windows;
-        // FP64 4-plane windows for the first pass (three CTAs an SM still
-        // fit without the solute windows), 3-plane for a pass with the solute
-        const int nslot = ctx->nslot ? ctx->nslot : ((is64(ctx) && nsw == 1) ? 3 : 4);
-        const int nslot_last = ctx->nslot ? ctx->nslot : (is64(ctx) ? 3 : 4);
+        const int nslot = ctx->nslot ? ctx->nslot : 3;
         auto tm_of = [ctx](const void* buf) -> const CUtensorMap& {
             return ctx->tmap[buf == ctx->tmap_buf[0] ? 0 : 1];
         };
@@ -683,9 +679,9 @@ static int one_step(pf_ctx* ctx)
             f2.phi_mid = cur;
             f2.phi_new = oth;
             if (ctx->ktiming) { e0 = new_event(); e1 = new_event(); cudaEventRecord(e0, ctx->stream); }
-            CK(is64(ctx) ? launch_march_last<double>(tm_of(cur), ctx->dd, s, f2, lanes, nslot_last, ctx->zchunk,
+            CK(is64(ctx) ? launch_march_last<double>(tm_of(cur), ctx->dd, s, f2, lanes, nslot, ctx->zchunk,
                                                      ctx->d_status, ctx->stream)
-                         : launch_march_last<float>(tm_of(cur), ctx->dd, s, f2, lanes, nslot_last, ctx->zchunk,
+                         : launch_march_last<float>(tm_of(cur), ctx->dd, s, f2, lanes, nslot, ctx->zchunk,
                                                     ctx->d_status, ctx->stream),
                "march last sweep + solute");
             if (ctx->ktiming) { cudaEventRecord(e1, ctx->stream); ctx->ev_last.push_back({e0, e1}); }

@@ -84,7 +84,7 @@ struct pf_batch {
     int tile_y = 8, zchunk = 64, n_sm = 0;   // persistent grids: n_sm x resident CTAs
     int pair = 0;                      // 32 x 8 tiles with two cells per thread (set by the autotuner)
     int march = 1;                     // TMA-staged march passes (32 x 8 tiles); 0: the cp.async passes
-    int nslot = 0;                     // node-window planes of the march passes (0: 3 in FP64, 4 in FP32)
+    int nslot = 0;                     // window mode of the march passes (0: 3)
     CUtensorMap* d_tmaps = nullptr;    // 2 per slot: the tensor maps of its phase-field buffers
     int* d_ctr = nullptr;              // work-item counters of a graph's launches (2 per step)
     int* d_status = nullptr;           // kernel status word (0, or the code a kernel left there)
@@ -175,7 +175,7 @@ static int capture_graph(pf_batch* b)
 {
     const bool smooth = any_smooth(b);
     const bool march = use_march(b);
-    const int nslot = b->nslot ? b->nslot : (b64(b) ? 3 : 4);
+    const int nslot = b->nslot ? b->nslot : 3;
     // two cells per thread on 32 x 8 tiles when the autotuner measured it
     // faster: the march passes in either precision (not with the smooth
     // noise); the cp.async passes in FP32 only, on decks without heat

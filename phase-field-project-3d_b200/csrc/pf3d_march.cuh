@@ -52,21 +52,27 @@ template <typename S> struct Lanes<S, 2> {
     static __device__ __forceinline__ S get(const V& v, int l) { return l ? v.y() : v.x(); }
 };
 
-// Window modes of the march passes:
-//   3: node / solute-point windows of 3 planes, two barriers per plane;
-//   4: windows of 4 planes, one barrier per plane;
+// Window modes of the march passes (one barrier per plane in each):
+//   3: node / solute-point windows of 3 planes.  The cells of plane z read
+//      plane z's nodes and points at their neighbours' positions, written
+//      by other threads before the previous plane's barrier, and those of
+//      planes z-1 and z+1 only at their own position, written by the same
+//      thread; so when the nodes of plane z+1 overwrite plane z-2's slot,
+//      the last cross-thread reader of that slot (the cells of plane z-2)
+//      is behind the previous plane's barrier, and no second barrier is
+//      needed;
+//   4: windows of 4 planes (a spare slot, same results);
 //   5: the own column's values rolled in registers along z -- the phase
 //      values of planes z-1, z, z+1 at the cell and its four axis
 //      neighbours, the cell's node quantities of planes z-1, z, z+1 and its
 //      solute-point quantities of the same planes -- so the stencil reads
 //      from shared memory only the in-plane neighbours of plane z (the
-//      diagonal phase values and the four neighbour nodes and points);
-//      windows of 3 planes then need one barrier per plane.
+//      diagonal phase values and the four neighbour nodes and points),
+//      with windows of 3 planes.
 template <int WIN> struct MarchWin {
     static_assert(WIN == 3 || WIN == 4 || WIN == 5, "window mode 3, 4 or 5");
     static constexpr int nslot = (WIN == 4) ? 4 : 3;
     static constexpr bool roll = WIN == 5;
-    static constexpr bool two_barriers = WIN == 3;
 };
 
 // Shared-memory layout of one tile (bytes from a 128-byte aligned base).
@@ -693,9 +699,7 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
         }
         s6 = s6p1;
         sn = snp1;
-        // window mode 3: the next plane's nodes overwrite plane z-1's slot
-        if constexpr (MarchWin<WIN>::two_barriers) __syncthreads();
-            zoff += pl;
+        zoff += pl;
         return true;
     };
     if constexpr (SPLIT) {
