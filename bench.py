@@ -328,7 +328,7 @@ def main():
     ap.add_argument("--no-error", action="store_true")
     ap.add_argument("--error-steps", type=int, default=2000)
     ap.add_argument("--serve-requests", type=int, default=2000)
-    ap.add_argument("--serve-step-scale", type=float, default=0.25)
+    ap.add_argument("--serve-step-scale", type=float, default=0.05)
     ap.add_argument("--serve-quantum", type=int, default=16)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
