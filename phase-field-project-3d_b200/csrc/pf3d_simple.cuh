@@ -168,41 +168,111 @@ struct KSum {
     }
 };
 
+// The grid walks 32 x 8-column tiles, each marched along z over a chunk of
+// kDiagZ planes (a persistent grid: block b takes tiles b, b + gridDim.x,
+// ...; the per-thread sums carry across its tiles, so the reduction order is
+// fixed by the launch shape).  The march goes in groups of kDiagG planes: a
+// thread first issues the reads of the whole group -- phi of the next
+// kDiagG planes and c, T, DPP of the group's planes, each cell read once from
+// HBM, all in flight together -- then shares the group's phase planes
+// through shared memory (one barrier a group) and evaluates its cells, with
+// the phase field of the planes above and below in registers (indexed at
+// compile time, so no register is moved before its load lands).  Only the
+// tile's edge cells read an in-plane neighbour from global memory (L2).  The
+// central gradient multiplies by the host-rounded 0.5/dx (within an ulp of
+// diag_body.inc's (a-b)*0.5d0/dx, far inside the sums' tolerance).  Within
+// a tile a thread sums its column's at most kDiagZ terms in plain FP64
+// (every term is nonnegative: phi^2, c and the energy density, so the
+// relative error stays below kDiagZ ulps) and adds the column sum to its
+// compensated (Neumaier) totals.
+constexpr int kDiagZ = 64;
+constexpr int kDiagG = 4;   // planes a group
 template <typename T>
-__global__ void __launch_bounds__(256) k_diag(DomainDesc d, const T* __restrict__ pn, const T* __restrict__ cn,
-                                              const T* __restrict__ tw, const T* __restrict__ dw,
-                                              double* __restrict__ part)
+__global__ void __launch_bounds__(256, 4) k_diag(DomainDesc d, const T* __restrict__ pn, const T* __restrict__ cn,
+                                                 const T* __restrict__ tw, const T* __restrict__ dw,
+                                                 double* __restrict__ part)
 {
-    const long long ncell = (long long)d.nx * d.ny * d.nz;
     KSum l2{0, 0}, sol{0, 0}, fe{0, 0};
     double mx = -DBL_MAX, mn = DBL_MAX, bad = 0.0;
-    const double dx = d.dx, dy = d.dy, dz = d.dz, E0 = d.E0, w0 = d.W0;
-    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
-        int x = (int)(q % d.nx);
-        long long r = q / d.nx;
-        int y = (int)(r % d.ny);
-        int z = (int)(r / d.ny);
-        long long id = cell_off(d, x, y, z);
-        double phi = (double)pn[id];
-        const double cv = (double)cn[id];
-        l2.add(phi * phi);
-        mx = nan_max(mx, phi);
-        mn = nan_min(mn, phi);
-        sol.add(cv);
-        bool fin = isfinite(phi) && isfinite(cv);
-        if (tw) fin = fin && isfinite((double)tw[id]);
-        if (dw) fin = fin && isfinite((double)dw[id]);
-        if (!fin) bad += 1.0;
-        double w_term = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(w0, phi), phi), 1.0 - phi), 1.0 - phi);
-        double grad2 = 0.0;
-        if (x > 0 && x < d.nx - 1 && y > 0 && y < d.ny - 1 && z > 0 && z < d.nz - 1) {
-            double gx = __dmul_rn((double)pn[id + 1] - (double)pn[id - 1], 0.5) / dx;
-            double gy = __dmul_rn((double)pn[id + d.px] - (double)pn[id - d.px], 0.5) / dy;
-            double gz = __dmul_rn((double)pn[id + d.plane] - (double)pn[id - d.plane], 0.5) / dz;
-            grad2 = __dadd_rn(__dadd_rn(__dmul_rn(gx, gx), __dmul_rn(gy, gy)), __dmul_rn(gz, gz));
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    const long long px = d.px, pl = d.plane;
+    const double dx = d.dx, dy = d.dy, dz = d.dz, w0 = d.W0, hx = d.hx, hy = d.hy, hz = d.hz;
+    const double hE2 = __dmul_rn(__dmul_rn(0.5, d.E0), d.E0);
+    __shared__ double sp[2][kDiagG][8][32];   // the group's phase planes, double-buffered by group parity
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int ntx = (nx + 31) >> 5, nty = (ny + 7) >> 3, ntz = (nz + kDiagZ - 1) / kDiagZ;
+    const long long ntiles = (long long)ntx * nty * ntz;
+    long long plk[kDiagG + 1];   // k planes, in elements
+#pragma unroll
+    for (int k = 0; k <= kDiagG; ++k) plk[k] = (long long)k * pl;
+    int g = 0;   // group parity across the whole walk
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int bx = (int)(t % ntx);
+        const long long r = t / ntx;
+        const int by = (int)(r % nty), bz = (int)(r / nty);
+        const int x = bx * 32 + tx, y = by * 8 + ty;
+        const bool own = x < nx && y < ny;
+        const bool xy_in = x > 0 && x < nx - 1 && y > 0 && y < ny - 1;
+        const int z0 = bz * kDiagZ, z1 = min(z0 + kDiagZ, nz);
+        const long long col = own ? (long long)x + (long long)y * px : 0;
+        // phase field of this column at planes z-1 (pprev) and z (pcur) of the group's first plane z
+        double pprev = (own && z0 > 0) ? (double)pn[col + (long long)(z0 - 1) * pl] : 0.0;
+        double pcur = own ? (double)pn[col + (long long)z0 * pl] : 0.0;
+        double s_l2 = 0.0, s_sol = 0.0, s_fe = 0.0;   // this column's sums over the chunk
+        for (int zb = z0; zb < z1; zb += kDiagG, g ^= 1) {
+            const int ng = min(kDiagG, z1 - zb);          // planes in this group (uniform)
+            const long long ib = col + (long long)zb * pl;
+            double pnx[kDiagG], cv[kDiagG], tv[kDiagG], dv[kDiagG];   // phi of plane zb+k+1; c, T, DPP of zb+k
+#pragma unroll
+            for (int k = 0; k < kDiagG; ++k) {
+                const bool in = own && k < ng;
+                pnx[k] = (in && zb + k + 1 < nz) ? (double)pn[ib + plk[k + 1]] : 0.0;
+                cv[k] = in ? (double)cn[ib + plk[k]] : 0.0;
+                tv[k] = (in && tw) ? (double)tw[ib + plk[k]] : 0.0;
+                dv[k] = (in && dw) ? (double)dw[ib + plk[k]] : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < kDiagG; ++k) sp[g][k][ty][tx] = (k == 0) ? pcur : pnx[k - 1];
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < kDiagG; ++k) {
+                if (k >= ng || !own) continue;
+                const int z = zb + k;
+                const double phi = (k == 0) ? pcur : pnx[k - 1];
+                const double pm = (k == 0) ? pprev : ((k == 1) ? pcur : pnx[k - 2]);
+                const double pp = pnx[k];
+                s_l2 += phi * phi;
+                mx = nan_max(mx, phi);
+                mn = nan_min(mn, phi);
+                s_sol += cv[k];
+                bool fin = isfinite(phi) && isfinite(cv[k]);
+                if (tw) fin = fin && isfinite(tv[k]);
+                if (dw) fin = fin && isfinite(dv[k]);
+                if (!fin) bad += 1.0;
+                const double w_term = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(w0, phi), phi), 1.0 - phi), 1.0 - phi);
+                double grad2 = 0.0;
+                if (xy_in && z > 0 && z < nz - 1) {
+                    const long long id = ib + plk[k];
+                    const double xp = tx < 31 ? sp[g][k][ty][tx + 1] : (double)pn[id + 1];
+                    const double xm = tx > 0 ? sp[g][k][ty][tx - 1] : (double)pn[id - 1];
+                    const double yp = ty < 7 ? sp[g][k][ty + 1][tx] : (double)pn[id + px];
+                    const double ym = ty > 0 ? sp[g][k][ty - 1][tx] : (double)pn[id - px];
+                    const double gx = __dmul_rn(xp - xm, hx);
+                    const double gy = __dmul_rn(yp - ym, hy);
+                    const double gz = __dmul_rn(pp - pm, hz);
+                    grad2 = __dadd_rn(__dadd_rn(__dmul_rn(gx, gx), __dmul_rn(gy, gy)), __dmul_rn(gz, gz));
+                }
+                const double e = __dadd_rn(__dmul_rn(hE2, grad2), w_term);
+                s_fe += __dmul_rn(__dmul_rn(__dmul_rn(e, dx), dy), dz);
+            }
+            if (ng == kDiagG) {   // the next group's planes z-1 and z (a short group ends the chunk)
+                pprev = pnx[kDiagG - 2];
+                pcur = pnx[kDiagG - 1];
+            }
         }
-        double e = __dadd_rn(__dmul_rn(__dmul_rn(__dmul_rn(0.5, E0), E0), grad2), w_term);
-        fe.add(__dmul_rn(__dmul_rn(__dmul_rn(e, dx), dy), dz));
+        l2.add(s_l2);
+        sol.add(s_sol);
+        fe.add(s_fe);
     }
     __shared__ double sh[8][9];
     double v[9] = {l2.s, l2.c, mx, mn, sol.s, sol.c, fe.s, fe.c, bad};
@@ -234,13 +304,15 @@ __global__ void __launch_bounds__(256) k_diag(DomainDesc d, const T* __restrict_
     }
 }
 
+// One warp merges the per-block partials: lane l takes blocks l, l + 32, ...,
+// then the lanes merge in a fixed shuffle order (deterministic).
 template <typename T>  // templated only so each precision unit owns its copy
 __global__ void k_diag_final(const double* __restrict__ part, int nblk, double* __restrict__ out)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
     KSum l2{0, 0}, sol{0, 0}, fe{0, 0};
     double mx = -DBL_MAX, mn = DBL_MAX, bad = 0.0;
-    for (int b = 0; b < nblk; ++b) {
+    for (int b = (int)threadIdx.x; b < nblk; b += 32) {
         const double* p = part + (long long)b * kDiagRow;
         l2.merge(p[0], p[1]);
         mx = nan_max(mx, p[2]);
@@ -249,12 +321,24 @@ __global__ void k_diag_final(const double* __restrict__ part, int nblk, double* 
         fe.merge(p[6], p[7]);
         bad += p[8];
     }
-    out[0] = sqrt(l2.s + l2.c);
-    out[1] = mx;
-    out[2] = mn;
-    out[3] = sol.s + sol.c;
-    out[4] = fe.s + fe.c;
-    out[5] = bad;   // cells with a non-finite phi or c (the watchdog)
+    double v[9] = {l2.s, l2.c, mx, mn, sol.s, sol.c, fe.s, fe.c, bad};
+    for (int off = 16; off > 0; off >>= 1) {
+        double o[9];
+        for (int q = 0; q < 9; ++q) o[q] = __shfl_down_sync(0xffffffffu, v[q], off);
+        KSum a{v[0], v[1]}; a.merge(o[0], o[1]); v[0] = a.s; v[1] = a.c;
+        v[2] = nan_max(v[2], o[2]); v[3] = nan_min(v[3], o[3]);
+        KSum b{v[4], v[5]}; b.merge(o[4], o[5]); v[4] = b.s; v[5] = b.c;
+        KSum e{v[6], v[7]}; e.merge(o[6], o[7]); v[6] = e.s; v[7] = e.c;
+        v[8] += o[8];
+    }
+    if (threadIdx.x == 0) {
+        out[0] = sqrt(v[0] + v[1]);
+        out[1] = v[2];
+        out[2] = v[3];
+        out[3] = v[4] + v[5];
+        out[4] = v[6] + v[7];
+        out[5] = v[8];   // cells with a non-finite phi, c, T or DPP (the watchdog)
+    }
 }
 
 // ---- host conversion staging (FP32 contexts) ----
