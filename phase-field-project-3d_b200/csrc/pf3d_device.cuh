@@ -9,7 +9,9 @@
 //            --fmad=false so no multiply-add is contracted, matching gfortran
 //            on x86-64.
 //   float  : storage and stencil arithmetic in FP32; the divisions by grid
-//            constants become multiplications by host-rounded reciprocals.
+//            constants become multiplications by host-rounded reciprocals,
+//            the others products with the hardware's approximate
+//            reciprocal, and log uses the hardware's approximate log2.
 //            Its error is stated against the FP64 form, not bit parity.
 #pragma once
 #include <cstdint>
@@ -207,10 +209,28 @@ template <> struct Ar<double> {
     static __device__ __forceinline__ double div(double a, double b) { return a * rcp_nr(b); }
     static __device__ __forceinline__ double lg(double x) { return pf_log(x); }
 };
+// FP32 fast form: the hardware's approximate reciprocal and base-2
+// logarithm (PTX rcp.approx.ftz.f32, lg2.approx.ftz.f32), a quotient as the
+// product with the reciprocal and ln x = log2(x) ln 2.  The lane pairs take
+// the same scalar steps lane by lane, so every lane of a pair gets the bits
+// of the one-cell form.
+__device__ __forceinline__ float rcp_ap(float x)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float lg2_ap(float x)
+{
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+constexpr float kLn2f = 0.693147180559945309f;   // ln 2 rounded to float
 template <> struct Ar<float> {
-    static __device__ __forceinline__ float rcp(float x) { return __fdividef(1.0f, x); }
-    static __device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
-    static __device__ __forceinline__ float lg(float x) { return __logf(x); }
+    static __device__ __forceinline__ float rcp(float x) { return rcp_ap(x); }
+    static __device__ __forceinline__ float div(float a, float b) { return __fmul_rn(a, rcp_ap(b)); }
+    static __device__ __forceinline__ float lg(float x) { return __fmul_rn(lg2_ap(x), kLn2f); }
 };
 
 // ---- lane-generic helpers: scalar float / double, and the lane pairs F2 / D2
@@ -246,9 +266,12 @@ PF3D_PAIR_SEL(sel_le, <=)
 #undef PF3D_PAIR_SEL
 
 template <> struct Ar<F2> {
-    static __device__ __forceinline__ F2 rcp(F2 x) { return F2(__fdividef(1.0f, x.x()), __fdividef(1.0f, x.y())); }
-    static __device__ __forceinline__ F2 div(F2 a, F2 b) { return F2(__fdividef(a.x(), b.x()), __fdividef(a.y(), b.y())); }
-    static __device__ __forceinline__ F2 lg(F2 x) { return F2(__logf(x.x()), __logf(x.y())); }
+    static __device__ __forceinline__ F2 rcp(F2 x) { return F2(rcp_ap(x.x()), rcp_ap(x.y())); }
+    static __device__ __forceinline__ F2 div(F2 a, F2 b)
+    {
+        return F2(Ar<float>::div(a.x(), b.x()), Ar<float>::div(a.y(), b.y()));
+    }
+    static __device__ __forceinline__ F2 lg(F2 x) { return F2(Ar<float>::lg(x.x()), Ar<float>::lg(x.y())); }
 };
 template <> struct Ar<D2> {
     static __device__ __forceinline__ D2 rcp(D2 x) { return D2(rcp_nr(x.a), rcp_nr(x.b)); }
