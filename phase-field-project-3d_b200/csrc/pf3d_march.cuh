@@ -723,12 +723,12 @@ __device__ __forceinline__ bool march_tile(const DomainDesc& d, const KC<S>& c, 
 // allows no more): FP64 3, or 2 -- 128 registers a thread -- for the rolled
 // window mode (its carried column values), a solute pass with 4-plane
 // windows and a pass that may draw the smooth noise (its trilinear blend of
-// eight hashes); FP32 pairs 5 for a pass with the heat equation, 4 otherwise
-// and in the rolled mode; FP32 single cells 3
+// eight hashes); FP32 pairs 6 (80 registers, no spills), 5 in the rolled
+// mode; FP32 single cells 3
 template <typename S, int L, int WIN, bool SOL, bool HEAT, bool SMOOTH = false>
 struct MarchOcc {
     static constexpr int v = (sizeof(S) == 8) ? ((WIN == 5 || (SOL && WIN == 4) || SMOOTH) ? 2 : 3)
-                                              : (L == 2 ? ((HEAT && WIN != 5) ? 6 : 5) : 3);
+                                              : (L == 2 ? ((WIN != 5) ? 6 : 5) : 3);
 };
 
 // single domain: one CTA per tile; the phase field comes through `tm`
