@@ -8,8 +8,9 @@ diagonal printed every 5000 steps to 45 000 as karma3d.f90:300-302 prints
 them (ponta_eixo = tip_x dx, ponta_diag = tip_d dx sqrt(3), F7.1).  This
 script steps the oracle from the program's seed (karma3d.f90:130-144) and
 compares every printed pair with the record; it exits non-zero on a
-mismatch.  About 75 minutes on 8 host threads (OMP_NUM_THREADS), so it is a
-script, not part of the test suite; tests/test_karma_record_gpu.py makes the
+mismatch.  About 100 minutes on 8 host threads (OMP_NUM_THREADS; measured:
+5916 s, all nine pairs equal to the record), so it is a script, not part of
+the test suite; tests/test_karma_record_gpu.py makes the
 same check of the GPU kernels in about 30 s.
 
     OMP_NUM_THREADS=8 python oracle/karma_record_check.py
